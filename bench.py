@@ -1,0 +1,389 @@
+"""Benchmark: Barnes-Hut steps on one B200 per rank (replicas), one JSON line.
+
+Workload (the large-scale configuration): gen_type shell, N = 1,048,576 on a
+sphere of radius 100, masses uniform in [5e10, 5e11], rotation 0.1 about z,
+size 1024, theta 0.5, adaptive dt (min_adaptive_dt 0.00333, max_pos_change 3,
+max_vel_change 3). A step is one full pass of the hot path on the GPU: root
+cube -> Morton keys -> radix sort -> octree -> mass/COM -> fused walk + gravity
+-> adaptive dt -> update.
+
+  value        interactions/s over K resident steps (inputs already in HBM),
+               CUDA events on the engine's stream, max over ranks
+  e2e          the same metric through the C ABI with host buffers: every step
+               uploads pos/vel/mass from pinned memory and downloads pos/vel
+  roofline     the fused walk kernel: 20 FLOP per interaction (the customary
+               N-body count) against the measured FP32 FMA peak
+  cpu_baseline the reference's own CPU walk (oracle/_ref, all host threads) on a
+               bounded sample of the same workload
+
+`--impl reference` times the reference's CPU implementation alone (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "interactions/s & steps/s, N=1M θ=0.5, p99 acc err≤1e-5 vs FP64; adjoint/fwd ratio"
+UNIT = "interactions/s"
+FLOP_PER_INTERACTION = 20
+WORKLOAD = dict(gen_type=2, n=1 << 20, r_sphere=100.0, rotation_magnitude=0.1, size=1024.0,
+                min_mass=5e10, max_mass=5e11, seed=0xDEADBEEF)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=WORKLOAD["n"])
+    ap.add_argument("--theta", type=float, default=0.5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU walk seconds of the sample")
+    return ap.parse_args()
+
+
+def workload_config(args) -> dict:
+    return {"workload": f"shell N={args.n} theta={args.theta} adaptive dt", "gen_type": "shell",
+            "n": args.n, "theta": args.theta, "r_sphere": 100.0, "size": 1024.0, "rotation_magnitude": 0.1,
+            "adaptive_dt": {"min_adaptive_dt": 0.00333, "max_pos_change": 3.0, "max_vel_change": 3.0},
+            "parallelism": f"replicas x{args.gpus}",
+            "l2": "working set (~300 MB per 1M particles) exceeds the 126 MB L2; no flush between steps"}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.p is not None:
+            time.sleep(0.25)
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                self.out = ""
+
+    def summary(self) -> dict:
+        rows = []
+        for line in (self.out or "").strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5], f[6], f[7], f[8]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            for name, v in zip(names, r[2:]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def cpu_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_reference_sample(pos, mass, theta, seconds, threads, counts=None):
+    """The reference's own CPU path (oracle/_ref) on a bounded sample: tree +
+    mass/COM over all N, the walk for a seeded sample of particles. Returns
+    (interactions/s, description, kind, per-step seconds)."""
+    import oracle
+    n = len(mass)
+    kind = "reference"
+    try:
+        R = oracle.Reference()
+    except FileNotFoundError:
+        R = None
+        kind = "port"
+    orc = oracle.Oracle()
+    rng = np.random.default_rng(0xDEADBEEF)
+    # calibrate the walk rate on 4096 particles
+    cal = np.sort(rng.choice(n, min(n, 4096), replace=False)).astype(np.uint32)
+    if R is not None:
+        _, t = R.forces_sample(pos, mass, cal, theta, threads=threads)
+    else:
+        t0 = time.perf_counter(); orc.forces(pos, mass, theta, threads=threads, sample=cal)
+        t = np.array([0.0, 0.0, time.perf_counter() - t0])
+    per = max(t[2], 1e-6) / len(cal)
+    m = int(min(n, max(4096, seconds / per)))
+    sample = np.sort(rng.choice(n, m, replace=False)).astype(np.uint32)
+    if counts is None:
+        _, cnt = orc.forces(pos, mass, theta, threads=threads, sample=sample)
+    else:
+        cnt = counts[sample]
+    inter = float(np.sum(cnt, dtype=np.float64))
+    if R is not None:
+        _, t = R.forces_sample(pos, mass, sample, theta, threads=threads)
+        build, com, walk = float(t[0]), float(t[1]), float(t[2])
+    else:
+        t0 = time.perf_counter()
+        orc.forces(pos, mass, theta, threads=threads, sample=sample)
+        build, com, walk = 0.0, 0.0, time.perf_counter() - t0
+    step_s = walk + (build + com) * m / n
+    desc = (f"{m} of {n} particles walked ({'reference barnes_hut_threaded' if R else 'oracle port'}, "
+            f"{threads} threads); tree build {build:.3f}s + mass/COM {com:.3f}s over all N amortised by {m}/{n}; "
+            f"walk {walk:.3f}s")
+    return inter / step_s, desc, kind, step_s
+
+
+def run_reference(args) -> None:
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    orc = oracle.Oracle()
+    g = oracle.GenParams(gen_type=2, size=1024.0, r_sphere=100.0, rotation_magnitude=0.1)
+    pos, vel, mass = orc.generate(g, args.n)
+    threads = cpu_cores()
+    seconds = max(1.0, min(args.cpu_seconds, 120.0 / max(1, args.steps + args.warmup)))
+    vals = []
+    desc, kind = "", "reference"
+    counts = None
+    for s in range(args.warmup + args.steps):
+        v, desc, kind, _ = cpu_reference_sample(pos, mass, args.theta, seconds, threads, counts)
+        if s >= args.warmup:
+            vals.append(v)
+    value = float(np.median(vals)) if vals else None
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded reference generator)",
+            "config": workload_config(args),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch
+    import nbodysim_b200 as nb
+    from nbodysim_b200 import build as nbbuild
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    nbbuild.build()
+    stream = torch.cuda.current_stream()
+    g = nb.gen_params(gen_type=2, size=1024.0, r_sphere=100.0, rotation_magnitude=0.1, seed=0xDEADBEEF + rank)
+    pos0, vel0, mass = nb.generate(args.n, g)
+    params = nb.default_params(theta=args.theta, adaptive=1, min_adaptive_dt=0.00333, max_pos_change=3.0,
+                               max_vel_change=3.0, device=local)
+    eng = nb.Engine(params)
+    eng._lib.nbody_set_stream(eng._h, C_void(stream.cuda_stream))
+
+    # ---- resident steps (device-timed)
+    eng.set_particles(pos0, vel0, mass)
+    eng.step(args.warmup)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    launches0 = eng.stats()["kernel_launches"]
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        ev0.record(stream)
+        eng.step(args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    st = eng.stats()
+    launches = st["kernel_launches"] - launches0
+    ms_total = ev0.elapsed_time(ev1)
+    inter_total = st["interactions_total"]
+    if pg:
+        t = torch.tensor([ms_total], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_total = float(t.item())
+        it = torch.tensor([float(inter_total)], device="cuda", dtype=torch.float64)
+        pg.all_reduce(it)
+        inter_all = float(it.item())
+    else:
+        inter_all = float(inter_total)
+    ms_step = ms_total / args.steps
+    value = inter_all / (ms_total * 1e-3)
+    steps_per_s = 1e3 / ms_step
+
+    # ---- per-phase times (CUDA events inside the engine, one step per call)
+    eng.set_timing(True)
+    ph = {"tree": [], "com": [], "walk": [], "update": [], "inter": []}
+    for _ in range(max(3, min(args.steps, 10))):
+        eng.step(1)
+        s = eng.stats()
+        ph["tree"].append(s["ms_tree"]); ph["com"].append(s["ms_com"])
+        ph["walk"].append(s["ms_walk"]); ph["update"].append(s["ms_update"])
+        ph["inter"].append(s["interactions"])
+    eng.set_timing(False)
+    walk_ms = float(np.mean(ph["walk"]))
+    walk_inter = float(np.mean(ph["inter"]))
+
+    # ---- e2e: host buffers through the C ABI every step
+    hp = torch.empty((args.n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    hv = torch.empty((args.n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    hm = torch.empty((args.n,), dtype=torch.float64, pin_memory=True).numpy()
+    hp[:] = pos0; hv[:] = vel0; hm[:] = mass
+    for _ in range(max(1, args.warmup // 2)):
+        eng.step_host(hp, hv, hm, 1)
+    hp[:] = pos0; hv[:] = vel0
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    inter_e2e = 0
+    e0.record(stream)
+    for _ in range(args.steps):
+        eng.step_host(hp, hv, hm, 1)
+        inter_e2e += eng.stats()["interactions_total"]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if pg:
+        t = torch.tensor([e2e_ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+        it = torch.tensor([float(inter_e2e)], device="cuda", dtype=torch.float64)
+        pg.all_reduce(it)
+        inter_e2e = float(it.item())
+    e2e_value = float(inter_e2e) / (e2e_ms * 1e-3)
+
+    if rank != 0:
+        eng.close()
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+
+    # ---- accuracy on the initial state: vs the FP64 form (same lists) and FP64 direct sum
+    acc_mixed, counts = eng.barnes_hut(pos0, mass, theta=args.theta, counts=True)
+    with nb.Engine(nb.default_params(theta=args.theta, precision=nb.PRECISION_FP64, device=local)) as e64:
+        acc64 = e64.barnes_hut(pos0, mass, theta=args.theta)
+        e64._lib.nbody_set_timing(e64._h, 1)
+        e64.barnes_hut(pos0, mass, theta=args.theta)
+        fp64_walk_ms = e64.stats()["ms_walk"]
+
+    def rel(a, b):
+        d = np.linalg.norm(b, axis=1)
+        return np.linalg.norm(a - b, axis=1) / np.where(d > 0, d, 1.0)
+
+    p99_vs_fp64 = float(np.percentile(rel(acc_mixed, acc64), 99))
+    direct = None
+    try:
+        import oracle
+        idx = np.random.default_rng(0xDEADBEEF).choice(args.n, 256, replace=False)
+        d = oracle.Oracle().direct(pos0, mass, targets=idx)
+        direct = {"p99_mixed": float(np.percentile(rel(acc_mixed[idx], d), 99)),
+                  "p99_fp64_bh": float(np.percentile(rel(acc64[idx], d), 99)),
+                  "sample": "256 particles, numpy default_rng(0xDEADBEEF)"}
+    except Exception as ex:  # the checker is optional here
+        direct = {"error": str(ex)}
+
+    # ---- roofline of the fused walk kernel
+    peak_tf, _ = nb.probe_fp32_peak(local)
+    achieved = FLOP_PER_INTERACTION * walk_inter / (walk_ms * 1e-3) / 1e12
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "walk_traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        try:
+            v, desc, kind, _ = cpu_reference_sample(pos0, mass, args.theta, args.cpu_seconds, cpu_cores(), counts)
+            cpu = {"value": v, "unit": UNIT, "cores": cpu_cores(), "kind": kind, "sample": desc}
+        except Exception as ex:
+            cpu = {"value": None, "unit": UNIT, "cores": cpu_cores(), "kind": "reference", "sample": f"failed: {ex}"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 pair forces + f64 tree/COM/state", "data": "synthetic (seeded reference generator)",
+        "config": workload_config(args),
+        "steps_per_s": steps_per_s * world,
+        "interactions_per_step": inter_all / args.steps / world,
+        "phases_ms": {k: float(np.mean(v)) for k, v in ph.items() if k != "inter"},
+        "walk_interactions_per_s": walk_inter / (walk_ms * 1e-3),
+        "fp64_form_walk_ms": fp64_walk_ms,
+        "p99_rel_err_vs_fp64_form": p99_vs_fp64,
+        "vs_fp64_direct_sum": direct,
+        "adjoint_fwd_ratio": None,
+        "clocks": clk.summary(),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 56 * args.n,
+                "d2h_bytes_per_step": 48 * args.n},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
+                     "frac": achieved / peak_tf if peak_tf else None, "traffic": traffic,
+                     "kernel": "k_walk (fused walk + gravity)",
+                     "peak_source": "measured FP32 FMA probe (nbody_probe_fp32_peak); MEASURED_PEAKS.json has no FP32 figure",
+                     "flop_per_interaction": FLOP_PER_INTERACTION},
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    eng.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def C_void(x):
+    import ctypes
+    return ctypes.c_void_p(x)
+
+
+def main() -> None:
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,172 @@
+/*
+ * nbody_b200 -- B200-native (sm_100a) Barnes-Hut engine: the C ABI.
+ *
+ * This library replaces the GPU force path of fosted3/nbodysim. The reference
+ * exposes it as a C++ call,
+ *     void barnes_hut_cuda(std::unordered_set<particle*>*, octree*, bool damping, datatype theta);
+ *                                                            (src/cuda_helper.h:8)
+ * backed by host-side tree walks and the chunk kernels behind run_compute
+ * (src/cuda_code.h:6-21). Here the whole step -- root cube, octree build,
+ * mass/centre-of-mass pass, per-particle walk + gravity, integration -- runs
+ * on the GPU. Every entry point takes plain pointers and sizes and returns a
+ * status code (0 = success) instead of exiting the process as the reference's
+ * handle_error does (src/cuda_code.cu:29-37).
+ *
+ * Layouts. Host arrays are array-of-structs triples: pos[3*i + k], k = x, y, z,
+ * in double precision (the reference's DOUBLE `datatype`, src/vector.h:4-13).
+ * Particle i of every input keeps index i in every output.
+ *
+ * Semantics (identical to the reference's CPU path, src/main.cpp:335-421):
+ *   root cube  = bbox midpoint, side = largest extent + 2 (ties: z extent)
+ *   octree     = one particle per leaf, octant bits x=1, y=2, z=4, strict '>'
+ *   open node  iff side / |com - x| > theta and the node is not a leaf
+ *   accept     otherwise, unless the node is the particle's own leaf
+ *   gravity    a += G M (com - x) / r^3, G = 6.67384e-11, no softening;
+ *              damping: |a| = G M / (r^2 + e^-r)
+ *   update     v += a dt; x += v dt
+ *
+ * Threading. A context belongs to one host thread at a time; all of its GPU
+ * work is ordered on its own stream. Separate contexts may run concurrently.
+ */
+#ifndef NBODY_B200_H
+#define NBODY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NBODY_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------- */
+#define NBODY_OK 0
+#define NBODY_ERR_INVALID 1      /* bad argument (null pointer, n too large, theta <= 0 ...) */
+#define NBODY_ERR_CUDA 2         /* a CUDA runtime call failed; see nbody_last_error_message */
+#define NBODY_ERR_OOM 3          /* device or pinned-host allocation failed */
+#define NBODY_ERR_COINCIDENT 4   /* two particles agree on all 63 octree levels; the reference
+                                    recurses without bound on such input (src/octree.cpp:173-195) */
+#define NBODY_ERR_NONFINITE 5    /* a position or mass is NaN or infinite */
+#define NBODY_ERR_CAPACITY 6     /* a walk's node stack exceeded its spill capacity */
+#define NBODY_ERR_NO_DEVICE 7    /* no CUDA device, or the device is not sm_100 */
+#define NBODY_ERR_STATE 8        /* call out of order (e.g. step before particles are set) */
+
+/* ---- configuration ---------------------------------------------------- */
+#define NBODY_PRECISION_MIXED 0  /* FP32 pair forces + FP32 accumulation; FP64 tree, COM, state */
+#define NBODY_PRECISION_FP64 1   /* the plain all-FP64 form of the same kernels */
+
+typedef struct nbody_params {
+    double theta;           /* opening angle, settings key `theta` (src/main.cpp:139) */
+    double dt;              /* time step, key `dt` (src/main.cpp:140) */
+    int damping;            /* key `damping` (src/main.cpp:127) */
+    int adaptive;           /* key `adaptive` (README.md:54; no reference code) */
+    double min_adaptive_dt; /* key `min_adaptive_dt` (README.md:56) */
+    double max_pos_change;  /* key `max_pos_change` (README.md:58) */
+    double max_vel_change;  /* key `max_vel_change` (README.md:60) */
+    int precision;          /* NBODY_PRECISION_* */
+    int device;             /* CUDA device ordinal */
+} nbody_params;
+
+/* Defaults of the reference's set_default (src/main.cpp:1312-1357) for the keys above;
+ * adaptive-dt defaults from README.md:54-60; precision MIXED; device 0. */
+void nbody_default_params(nbody_params *p);
+
+typedef struct nbody_ctx nbody_ctx;
+
+int nbody_create(const nbody_params *p, nbody_ctx **out);
+int nbody_destroy(nbody_ctx *ctx);
+int nbody_set_params(nbody_ctx *ctx, const nbody_params *p);
+/* Optional: order this context's GPU work on a caller-owned cudaStream_t. */
+int nbody_set_stream(nbody_ctx *ctx, void *cuda_stream);
+
+/* ---- the drop-in force call -------------------------------------------
+ * Replaces barnes_hut_cuda (src/cuda_helper.h:8, src/cuda_helper.cpp:218-246):
+ * given n positions and masses (host memory), overwrite acc_out (host, n x 3)
+ * with the Barnes-Hut acceleration of every particle. `damping` and `theta`
+ * are the call's arguments exactly as in the reference signature; the
+ * context's own values are not used. counts_out (optional, n) receives the
+ * number of accepted nodes per particle. */
+int nbody_barnes_hut(nbody_ctx *ctx, uint32_t n, const double *pos, const double *mass,
+                     int damping, double theta, double *acc_out, uint32_t *counts_out);
+
+/* ---- resident state ----------------------------------------------------
+ * The frame loop of src/main.cpp:1420-1492 restricted to the hot path, with
+ * the particle state kept in device memory between steps. */
+int nbody_set_particles(nbody_ctx *ctx, uint32_t n, const double *pos, const double *vel,
+                        const double *mass);
+/* Any output pointer may be NULL. acc is the last computed acceleration. */
+int nbody_get_particles(nbody_ctx *ctx, double *pos, double *vel, double *acc);
+/* nsteps full steps: root cube -> octree -> mass/COM -> walk+force -> (adaptive dt) -> update. */
+int nbody_step(nbody_ctx *ctx, uint32_t nsteps);
+/* Forces only, on the resident state (acc stays on the device). */
+int nbody_compute_forces(nbody_ctx *ctx);
+/* One step with host buffers in and out: upload pos/vel/mass, step, download pos/vel.
+ * pos/vel are updated in place. */
+int nbody_step_host(nbody_ctx *ctx, uint32_t n, double *pos, double *vel, const double *mass,
+                    uint32_t nsteps);
+
+/* Device addresses of the resident state (for zero-copy interop). Layout:
+ * pos, vel: n x double3 (AoS); mass: n doubles; acc: n x float3 (MIXED) or
+ * n x double3 (FP64). */
+typedef struct nbody_device_view {
+    uint32_t n;
+    void *pos, *vel, *mass, *acc;
+    int acc_is_double;
+} nbody_device_view;
+int nbody_device_view_get(nbody_ctx *ctx, nbody_device_view *out);
+
+/* ---- statistics and diagnostics ---------------------------------------- */
+typedef struct nbody_stats {
+    uint64_t interactions;   /* accepted (particle, node) pairs in the last force pass */
+    uint64_t interactions_total; /* summed over every pass of the last API call */
+    uint64_t kernel_launches;    /* kernels this context has enqueued since creation */
+    uint32_t tree_nodes;     /* internal nodes of the (chain-free) octree */
+    uint32_t tree_depth;     /* deepest internal-node level */
+    uint32_t max_stack;      /* deepest walk stack seen (entries) */
+    uint32_t fallback_tests; /* opening tests settled by the exact FP64 path */
+    double last_dt;          /* dt used by the last step */
+    double root_center[3];
+    double root_side;
+    float ms_tree, ms_com, ms_walk, ms_update; /* last pass, CUDA events; 0 if not timed */
+} nbody_stats;
+int nbody_get_stats(nbody_ctx *ctx, nbody_stats *out);
+/* Time phases with CUDA events on the context stream (default off). */
+int nbody_set_timing(nbody_ctx *ctx, int enabled);
+
+typedef struct nbody_diagnostics {
+    double kinetic;          /* sum 1/2 m v^2 */
+    double potential;        /* 1/2 sum_i m_i phi_i over the Barnes-Hut walk */
+    double momentum[3];      /* sum m v */
+    double angular_momentum[3]; /* sum m x cross v */
+    double mass;             /* total mass */
+    double com[3];           /* centre of mass */
+} nbody_diagnostics;
+/* Energies and momenta of the resident state (FP64 reductions). Runs one
+ * extra force pass with potentials. */
+int nbody_get_diagnostics(nbody_ctx *ctx, nbody_diagnostics *out);
+
+/* ---- initial conditions ----------------------------------------------
+ * Seeded generator of src/main.cpp:184-275 (std::default_random_engine, the
+ * same draw order), so a seed gives the reference's particles bit for bit. */
+typedef struct nbody_gen_params {
+    int gen_type;    /* 0 cube, 1 sphere, 2 shell  (key gen_type) */
+    int mass_dist;   /* 0 linear, 1 exp, 2 normal  (key mass_dist) */
+    int vel_dist;    /* key vel_dist */
+    double size, min_mass, max_mass, min_vel, max_vel, r_sphere, rotation_magnitude;
+    double rotation_vector[3];
+    double scale[3];
+    uint64_t seed;
+} nbody_gen_params;
+void nbody_default_gen_params(nbody_gen_params *g);
+int nbody_generate(const nbody_gen_params *g, uint32_t n, double *pos, double *vel, double *mass);
+
+/* ---- errors ------------------------------------------------------------ */
+const char *nbody_status_string(int status);
+/* Thread-local text of the last failure (CUDA error string or argument check). */
+const char *nbody_last_error_message(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NBODY_B200_H */

@@ -1,0 +1,328 @@
+"""nbodysim_b200 -- B200-native Barnes-Hut engine for fosted3/nbodysim's hot path.
+
+Python mirror of the library's C ABI (``include/nbody_b200.h``), loaded with
+ctypes from the in-tree ``nbodysim_b200/lib/libnbody_b200.so``. There is no CPU
+fallback: if the library is missing or no sm_100 GPU is present, calls raise.
+
+Reference interfaces mirrored here:
+
+* ``Engine.barnes_hut(pos, mass, damping, theta)`` -- ``barnes_hut_cuda(particles,
+  root, damping, theta)`` (src/cuda_helper.h:8): overwrites every particle's
+  acceleration with the Barnes-Hut sum.
+* ``Engine.step`` -- the frame loop's build -> mass -> com -> force -> update
+  (src/main.cpp:1420-1492) on resident device state.
+* ``Settings`` / ``read_settings`` / ``set_default`` -- the reference's config
+  struct, parser and defaults (src/main.cpp:115-160, 1123-1357).
+* ``generate`` -- ``generate_particle`` (src/main.cpp:226-275), seeded.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+from .settings import Settings, read_settings, set_default  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libnbody_b200.so")
+
+OK = 0
+ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_COINCIDENT, ERR_NONFINITE, ERR_CAPACITY, ERR_NO_DEVICE, ERR_STATE = range(1, 9)
+PRECISION_MIXED, PRECISION_FP64 = 0, 1
+CUBE, SPHERE, SHELL = 0, 1, 2
+LINEAR, EXP, NORMAL = 0, 1, 2
+
+
+class NBodyError(RuntimeError):
+    """A non-zero status from the C ABI."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("theta", C.c_double), ("dt", C.c_double), ("damping", C.c_int), ("adaptive", C.c_int),
+        ("min_adaptive_dt", C.c_double), ("max_pos_change", C.c_double), ("max_vel_change", C.c_double),
+        ("precision", C.c_int), ("device", C.c_int),
+    ]
+
+
+class GenParams(C.Structure):
+    _fields_ = [
+        ("gen_type", C.c_int), ("mass_dist", C.c_int), ("vel_dist", C.c_int),
+        ("size", C.c_double), ("min_mass", C.c_double), ("max_mass", C.c_double),
+        ("min_vel", C.c_double), ("max_vel", C.c_double), ("r_sphere", C.c_double),
+        ("rotation_magnitude", C.c_double), ("rotation_vector", C.c_double * 3),
+        ("scale", C.c_double * 3), ("seed", C.c_uint64),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("interactions", C.c_uint64), ("interactions_total", C.c_uint64), ("kernel_launches", C.c_uint64),
+        ("tree_nodes", C.c_uint32), ("tree_depth", C.c_uint32),
+        ("max_stack", C.c_uint32), ("fallback_tests", C.c_uint32), ("last_dt", C.c_double),
+        ("root_center", C.c_double * 3), ("root_side", C.c_double),
+        ("ms_tree", C.c_float), ("ms_com", C.c_float), ("ms_walk", C.c_float), ("ms_update", C.c_float),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["root_center"] = tuple(self.root_center)
+        return d
+
+
+class Diagnostics(C.Structure):
+    _fields_ = [
+        ("kinetic", C.c_double), ("potential", C.c_double), ("momentum", C.c_double * 3),
+        ("angular_momentum", C.c_double * 3), ("mass", C.c_double), ("com", C.c_double * 3),
+    ]
+
+    def as_dict(self) -> dict:
+        return dict(kinetic=self.kinetic, potential=self.potential, energy=self.kinetic + self.potential,
+                    momentum=tuple(self.momentum), angular_momentum=tuple(self.angular_momentum),
+                    mass=self.mass, com=tuple(self.com))
+
+
+class DeviceView(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("pos", C.c_void_p), ("vel", C.c_void_p), ("mass", C.c_void_p),
+                ("acc", C.c_void_p), ("acc_is_double", C.c_int)]
+
+
+# Every entry point of include/nbody_b200.h with its ctypes signature.
+_SIGS = {
+    "nbody_default_params": (None, [C.POINTER(Params)]),
+    "nbody_create": (C.c_int, [C.POINTER(Params), C.POINTER(C.c_void_p)]),
+    "nbody_destroy": (C.c_int, [C.c_void_p]),
+    "nbody_set_params": (C.c_int, [C.c_void_p, C.POINTER(Params)]),
+    "nbody_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "nbody_barnes_hut": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int, C.c_double,
+                                   C.c_void_p, C.c_void_p]),
+    "nbody_set_particles": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "nbody_get_particles": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "nbody_step": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "nbody_compute_forces": (C.c_int, [C.c_void_p]),
+    "nbody_step_host": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
+    "nbody_device_view_get": (C.c_int, [C.c_void_p, C.POINTER(DeviceView)]),
+    "nbody_get_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
+    "nbody_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "nbody_get_diagnostics": (C.c_int, [C.c_void_p, C.POINTER(Diagnostics)]),
+    "nbody_default_gen_params": (None, [C.POINTER(GenParams)]),
+    "nbody_generate": (C.c_int, [C.POINTER(GenParams), C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "nbody_status_string": (C.c_char_p, [C.c_int]),
+    "nbody_last_error_message": (C.c_char_p, []),
+    "nbody_probe_fp32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+}
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python -m nbodysim_b200.build` "
+                          "(there is no CPU fallback)")
+    lib = C.CDLL(path)
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(status: int) -> None:
+    if status != OK:
+        lib = load_library()
+        msg = lib.nbody_last_error_message().decode(errors="replace")
+        raise NBodyError(status, f"{lib.nbody_status_string(status).decode()}: {msg}")
+
+
+def _aos(a, n=None) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.ndim != 2 or a.shape[1] != 3 or (n is not None and a.shape[0] != n):
+        raise ValueError("expected an (n, 3) array")
+    return a
+
+
+def _vec(a, n) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+    if a.shape[0] != n:
+        raise ValueError("expected n masses")
+    return a
+
+
+def _ptr(a):
+    return a.ctypes.data if a is not None else None
+
+
+def default_params(**kw) -> Params:
+    p = Params()
+    load_library().nbody_default_params(C.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise AttributeError(k)
+        setattr(p, k, v)
+    return p
+
+
+def params_from_settings(s: Settings, **kw) -> Params:
+    """Engine parameters from the reference's config keys."""
+    return default_params(theta=s.theta, dt=s.dt, damping=int(s.damping), adaptive=int(s.adaptive),
+                          min_adaptive_dt=s.min_adaptive_dt, max_pos_change=s.max_pos_change,
+                          max_vel_change=s.max_vel_change, **kw)
+
+
+def gen_params(**kw) -> GenParams:
+    g = GenParams()
+    load_library().nbody_default_gen_params(C.byref(g))
+    for k, v in kw.items():
+        if k in ("rotation_vector", "scale"):
+            getattr(g, k)[:] = [float(x) for x in v]
+        else:
+            setattr(g, k, v)
+    return g
+
+
+def gen_params_from_settings(s: Settings) -> GenParams:
+    return gen_params(gen_type=s.gen_type, mass_dist=s.mass_dist, vel_dist=s.vel_dist, size=s.size,
+                      min_mass=s.min_mass, max_mass=s.max_mass, min_vel=s.min_vel, max_vel=s.max_vel,
+                      r_sphere=s.r_sphere, rotation_magnitude=s.rotation_magnitude,
+                      rotation_vector=s.rotation_vector, scale=(s.scale_x, s.scale_y, s.scale_z),
+                      seed=s.seed)
+
+
+def generate(n: int, g: GenParams | None = None, **kw):
+    """Seeded initial conditions: (pos (n,3), vel (n,3), mass (n,)), host arrays."""
+    g = g if g is not None else gen_params(**kw)
+    pos = np.zeros((n, 3)); vel = np.zeros((n, 3)); mass = np.zeros(n)
+    _check(load_library().nbody_generate(C.byref(g), n, pos.ctypes.data, vel.ctypes.data, mass.ctypes.data))
+    return pos, vel, mass
+
+
+class Engine:
+    """One device context (include/nbody_b200.h `nbody_ctx`)."""
+
+    def __init__(self, params: Params | None = None, **kw):
+        lib = load_library()
+        self._lib = lib
+        self.params = params if params is not None else default_params(**kw)
+        h = C.c_void_p()
+        _check(lib.nbody_create(C.byref(self.params), C.byref(h)))
+        self._h = h
+        self.n = 0
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.nbody_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_params(self, **kw) -> None:
+        for k, v in kw.items():
+            setattr(self.params, k, v)
+        _check(self._lib.nbody_set_params(self._h, C.byref(self.params)))
+
+    def set_timing(self, on: bool = True) -> None:
+        _check(self._lib.nbody_set_timing(self._h, int(on)))
+
+    def barnes_hut(self, pos, mass, damping: bool = False, theta: float = 0.5, counts: bool = False):
+        """Accelerations (n, 3) of every particle (the reference's barnes_hut_cuda)."""
+        pos = _aos(pos)
+        n = pos.shape[0]
+        mass = _vec(mass, n)
+        acc = np.zeros((n, 3))
+        cnt = np.zeros(n, np.uint32) if counts else None
+        _check(self._lib.nbody_barnes_hut(self._h, n, pos.ctypes.data, mass.ctypes.data, int(damping),
+                                          float(theta), acc.ctypes.data, _ptr(cnt)))
+        return (acc, cnt) if counts else acc
+
+    def set_particles(self, pos, vel, mass) -> None:
+        pos = _aos(pos)
+        n = pos.shape[0]
+        vel = _aos(vel, n) if vel is not None else None
+        mass = _vec(mass, n)
+        _check(self._lib.nbody_set_particles(self._h, n, pos.ctypes.data, _ptr(vel), mass.ctypes.data))
+        self.n = n
+
+    def get_particles(self, acc: bool = False):
+        pos = np.zeros((self.n, 3)); vel = np.zeros((self.n, 3))
+        a = np.zeros((self.n, 3)) if acc else None
+        _check(self._lib.nbody_get_particles(self._h, pos.ctypes.data, vel.ctypes.data, _ptr(a)))
+        return (pos, vel, a) if acc else (pos, vel)
+
+    def step(self, nsteps: int = 1) -> None:
+        _check(self._lib.nbody_step(self._h, nsteps))
+
+    def compute_forces(self) -> None:
+        _check(self._lib.nbody_compute_forces(self._h))
+
+    def step_host(self, pos, vel, mass, nsteps: int = 1):
+        """Steps host arrays in place (upload, nsteps, download). Returns (pos, vel)."""
+        n = pos.shape[0]
+        if pos.dtype != np.float64 or not pos.flags.c_contiguous or vel.dtype != np.float64 \
+                or not vel.flags.c_contiguous:
+            raise ValueError("pos/vel must be C-contiguous float64 (n, 3) arrays (updated in place)")
+        mass = _vec(mass, n)
+        _check(self._lib.nbody_step_host(self._h, n, pos.ctypes.data, vel.ctypes.data, mass.ctypes.data, nsteps))
+        self.n = n
+        return pos, vel
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(self._lib.nbody_get_stats(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def diagnostics(self) -> dict:
+        d = Diagnostics()
+        _check(self._lib.nbody_get_diagnostics(self._h, C.byref(d)))
+        return d.as_dict()
+
+    def device_view(self) -> DeviceView:
+        v = DeviceView()
+        _check(self._lib.nbody_device_view_get(self._h, C.byref(v)))
+        return v
+
+
+def probe_fp32_peak(device: int = 0) -> tuple[float, float]:
+    """Measured FP32 FMA throughput (TFLOP/s) and the probe kernel's time (ms)."""
+    tf = C.c_double(); ms = C.c_double()
+    _check(load_library().nbody_probe_fp32_peak(device, C.byref(tf), C.byref(ms)))
+    return tf.value, ms.value
+
+
+def header_symbols(path: str | None = None) -> list[str]:
+    """Names of the functions declared in include/*.h."""
+    import glob
+    import re
+    inc = os.path.join(os.path.dirname(HERE), "include")
+    paths = [path] if path else sorted(glob.glob(os.path.join(inc, "*.h")))
+    names = set()
+    for p in paths:
+        names |= set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(nbody_\w+)\s*\(", open(p).read(), re.M))
+    return sorted(names)
+
+
+__all__ = ["Engine", "NBodyError", "Params", "GenParams", "Settings", "read_settings", "set_default",
+           "generate", "gen_params", "default_params", "load_library", "params_from_settings",
+           "gen_params_from_settings", "header_symbols"]
+if sys.version_info < (3, 9):  # pragma: no cover
+    raise ImportError("python >= 3.9 required")

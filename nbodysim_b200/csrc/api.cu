@@ -1,0 +1,533 @@
+// The C ABI (include/nbody_b200.h): contexts, device arena, pass sequencing.
+//
+// One pass over the hot path, all on the context's stream:
+//   reset scalars -> root cube + keys + radix sort + octree (tree.cu)
+//   -> bottom-up mass/COM (tree.cu) -> fused walk + gravity (walk.cu)
+//   -> [update (step.cu)]
+// The reference does the tree and the walk on the host and ships per-chunk
+// interaction lists to the GPU every frame (src/cuda_helper.cpp:46-216); here
+// nothing but the inputs and the results crosses PCIe, and device memory is a
+// grow-only arena reused across calls (no per-call allocation after warm-up,
+// in place of the reference's per-call cudaMalloc/cudaFree and cudaDeviceReset,
+// src/cuda_code.cu:138-229).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "../../include/nbody_b200.h"
+#include "step.cuh"
+#include "tree.cuh"
+#include "walk.cuh"
+
+using namespace nbody;
+
+namespace {
+
+thread_local char g_msg[512] = "";
+
+int fail(int code, const char *fmt, const char *detail = "") {
+    std::snprintf(g_msg, sizeof g_msg, fmt, detail);
+    return code;
+}
+
+#define NB_CUDA(call)                                                                       \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess) {                                                            \
+            std::snprintf(g_msg, sizeof g_msg, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                          __FILE__, __LINE__);                                              \
+            return e_ == cudaErrorMemoryAllocation ? NBODY_ERR_OOM : NBODY_ERR_CUDA;         \
+        }                                                                                   \
+    } while (0)
+
+constexpr uint32_t kMaxParticles = 1u << 28;
+constexpr uint32_t kSpillCap = 4096;  // entries per walk warp
+constexpr unsigned kBboxBlocks = 592;
+constexpr unsigned kDiagBlocks = 296;
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+struct nbody_ctx {
+    nbody_params p;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    uint32_t cap = 0, n = 0;
+    bool have_state = false, have_vel = false, have_acc = false;
+    // arena
+    void *arena = nullptr;
+    size_t arena_bytes = 0;
+    double *pos = nullptr, *vel = nullptr, *mass = nullptr, *pot = nullptr, *acc_out = nullptr;
+    void *acc = nullptr;  // float3 (MIXED) / double3 (FP64), user order
+    uint32_t *counts = nullptr;
+    TreeBuild tb{};
+    double *diag_partial = nullptr;
+    int2 *spill = nullptr;
+    DevScalars *sc = nullptr;   // device
+    DevScalars *hsc = nullptr;  // pinned mirror
+    WalkLaunch wl_mixed{}, wl_fp64{};
+    int timing = 0;
+    cudaEvent_t ev[5] = {};
+    nbody_stats stats{};
+    unsigned long long launches = 0;  // kernels enqueued by this context
+};
+
+namespace {
+
+int set_device(nbody_ctx *c) {
+    NB_CUDA(cudaSetDevice(c->p.device));
+    return NBODY_OK;
+}
+
+int check_params(const nbody_params *p) {
+    if (!p) return fail(NBODY_ERR_INVALID, "params is null%s");
+    if (!(p->theta > 0.0) || !std::isfinite(p->theta)) return fail(NBODY_ERR_INVALID, "theta must be finite and > 0%s");
+    if (!std::isfinite(p->dt)) return fail(NBODY_ERR_INVALID, "dt must be finite%s");
+    if (p->precision != NBODY_PRECISION_MIXED && p->precision != NBODY_PRECISION_FP64)
+        return fail(NBODY_ERR_INVALID, "unknown precision%s");
+    if (p->adaptive && (!(p->max_pos_change > 0) || !(p->max_vel_change > 0) || !(p->min_adaptive_dt >= 0)))
+        return fail(NBODY_ERR_INVALID, "adaptive dt needs max_pos_change > 0, max_vel_change > 0, min_adaptive_dt >= 0%s");
+    return NBODY_OK;
+}
+
+// Carves every per-particle buffer out of one allocation sized for `cap`.
+int reserve(nbody_ctx *c, uint32_t n) {
+    if (n <= c->cap && c->arena) return NBODY_OK;
+    uint32_t cap = n < 1024 ? 1024 : n + n / 4;
+    if (cap > kMaxParticles) cap = kMaxParticles;
+    const size_t N = cap;
+    const size_t sort_blocks = (N + 4095) / 4096;
+    const size_t scan_tiles = (256 * sort_blocks + 4095) / 4096 + (N + 4095) / 4096 + 8;
+    const size_t spill_entries = (size_t)(c->wl_mixed.blocks > c->wl_fp64.blocks ? c->wl_mixed.blocks
+                                                                                   : c->wl_fp64.blocks) *
+                                 kWalkWarps * kSpillCap;
+    struct Piece { void **dst; size_t bytes; };
+    TreeBuild &tb = c->tb;
+    Piece pieces[] = {
+        {(void **)&c->pos, 24 * N}, {(void **)&c->vel, 24 * N}, {(void **)&c->mass, 8 * N},
+        {(void **)&c->acc, 24 * N}, {(void **)&c->acc_out, 24 * N}, {(void **)&c->counts, 4 * N},
+        {(void **)&c->pot, 8 * N},
+        {(void **)&tb.key_a, 8 * N}, {(void **)&tb.key_b, 8 * N}, {(void **)&tb.key2, 8 * N},
+        {(void **)&tb.key3, 8 * N}, {(void **)&tb.idx_a, 4 * N}, {(void **)&tb.idx_b, 4 * N},
+        {(void **)&tb.sort_hist, 4 * 256 * sort_blocks}, {(void **)&tb.scan_tmp, 4 * scan_tiles},
+        {(void **)&tb.body, 32 * N}, {(void **)&tb.onode, 32 * N},
+        {(void **)&tb.bleft, 4 * N}, {(void **)&tb.bright, 4 * N}, {(void **)&tb.bparent, 4 * N},
+        {(void **)&tb.leaf_bparent, 4 * N}, {(void **)&tb.bdelta, 4 * N},
+        {(void **)&tb.head_flag, 4 * N}, {(void **)&tb.head_id, 4 * N}, {(void **)&tb.ocount, 4 * N},
+        {(void **)&tb.ochild, 32 * N}, {(void **)&tb.ometa, 4 * N}, {(void **)&tb.oparent, 4 * N},
+        {(void **)&tb.leaf_oparent, 4 * N},
+        {(void **)&tb.bbox_partial, 8 * 7 * kBboxBlocks}, {(void **)&c->diag_partial, 8 * kDiagCount * kDiagBlocks},
+        {(void **)&c->spill, 8 * spill_entries},
+    };
+    size_t total = 0;
+    for (auto &pc : pieces) total += align256(pc.bytes);
+    if (c->arena) {
+        NB_CUDA(cudaStreamSynchronize(c->stream));
+        NB_CUDA(cudaFree(c->arena));
+        c->arena = nullptr;
+        c->cap = 0;
+    }
+    void *arena = nullptr;
+    cudaError_t e = cudaMalloc(&arena, total);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(NBODY_ERR_OOM, "device arena allocation failed (%s)", cudaGetErrorString(e));
+    }
+    char *p = (char *)arena;
+    for (auto &pc : pieces) {
+        *pc.dst = p;
+        p += align256(pc.bytes);
+    }
+    c->arena = arena;
+    c->arena_bytes = total;
+    c->cap = cap;
+    tb.bbox_blocks = kBboxBlocks;
+    tb.sc = c->sc;
+    c->have_state = c->have_vel = c->have_acc = false;
+    return NBODY_OK;
+}
+
+int check_status(nbody_ctx *c) {
+    NB_CUDA(cudaStreamSynchronize(c->stream));
+    const DevScalars &h = *c->hsc;
+    nbody_stats &s = c->stats;
+    s.interactions = h.interactions;
+    s.interactions_total = h.interactions_total;
+    s.kernel_launches = c->launches;
+    s.tree_nodes = h.n_onodes;
+    s.tree_depth = h.depth;
+    s.max_stack = h.max_stack;
+    s.fallback_tests = h.fallback_tests;
+    s.last_dt = h.dt_used;
+    for (int k = 0; k < 3; k++) s.root_center[k] = h.root_center[k];
+    s.root_side = h.root_side;
+    if (c->timing) {
+        float ms[4] = {0, 0, 0, 0};
+        for (int k = 0; k < 4; k++) cudaEventElapsedTime(&ms[k], c->ev[k], c->ev[k + 1]);
+        cudaGetLastError();  // an unrecorded event must not leak into later checks
+        s.ms_tree = ms[0]; s.ms_com = ms[1]; s.ms_walk = ms[2]; s.ms_update = ms[3];
+    }
+    if (h.status & kStatusNonFinite) return fail(NBODY_ERR_NONFINITE, "a position or mass is NaN or infinite%s");
+    if (h.status & kStatusCoincident)
+        return fail(NBODY_ERR_COINCIDENT, "particles coincide to 63 octree levels (the reference recurses without bound)%s");
+    if (h.status & kStatusCapacity) return fail(NBODY_ERR_CAPACITY, "walk stack spill capacity exceeded%s");
+    return NBODY_OK;
+}
+
+void tree_inputs(nbody_ctx *c, uint32_t n, bool want_vmax) {
+    TreeBuild &tb = c->tb;
+    tb.n = n;
+    tb.pos = c->pos;
+    tb.mass = c->mass;
+    tb.vel_for_max = want_vmax ? c->vel : nullptr;
+    tb.sc = c->sc;
+}
+
+void ev(nbody_ctx *c, int k) {
+    if (c->timing) cudaEventRecord(c->ev[k], c->stream);
+}
+
+// One force pass on the resident pos/mass: tree, COM, walk. Asynchronous.
+int force_pass(nbody_ctx *c, int damping, double theta, bool fp64, bool want_vmax, bool track_amax,
+               bool want_counts, bool want_pot) {
+    const uint32_t n = c->n;
+    unsigned launches = 1;
+    NB_CUDA(launch_reset_pass(c->sc, c->stream));
+    tree_inputs(c, n, want_vmax);
+    ev(c, 0);
+    NB_CUDA(build_octree(c->tb, c->stream, &launches));
+    ev(c, 1);
+    NB_CUDA(compute_com(c->tb, c->stream, &launches));
+    ev(c, 2);
+    WalkArgs a{};
+    a.t.n = n;
+    a.t.body = c->tb.body;
+    a.t.sidx = c->tb.idx_a;
+    a.t.onode = c->tb.onode;
+    a.t.ochild = c->tb.ochild;
+    a.t.ometa = c->tb.ometa;
+    a.t.sc = c->sc;
+    a.theta = theta;
+    a.damping = damping;
+    a.accf = fp64 ? nullptr : (float *)c->acc;
+    a.accd = fp64 ? (double *)c->acc : nullptr;
+    a.counts = want_counts ? c->counts : nullptr;
+    a.pot = want_pot ? c->pot : nullptr;
+    a.spill = c->spill;
+    a.spill_cap = kSpillCap;
+    a.n_groups = (n + 31) / 32;
+    a.track_max_acc = track_amax ? 1 : 0;
+    if (n > 0) {
+        NB_CUDA(launch_walk(a, fp64, fp64 ? c->wl_fp64 : c->wl_mixed, c->stream));
+        launches++;
+    }
+    c->launches += launches;
+    ev(c, 3);
+    c->have_acc = true;
+    return NBODY_OK;
+}
+
+// Clears the per-call status bits and the per-call interaction total.
+int begin_call(nbody_ctx *c) {
+    NB_CUDA(cudaMemsetAsync(&c->sc->status, 0, sizeof(uint32_t), c->stream));
+    NB_CUDA(cudaMemsetAsync(&c->sc->interactions_total, 0, sizeof(unsigned long long), c->stream));
+    return NBODY_OK;
+}
+
+int copy_scalars_back(nbody_ctx *c) {
+    NB_CUDA(cudaMemcpyAsync(c->hsc, c->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
+    return NBODY_OK;
+}
+
+int upload(nbody_ctx *c, uint32_t n, const double *pos, const double *vel, const double *mass) {
+    int rc = reserve(c, n);
+    if (rc) return rc;
+    NB_CUDA(cudaMemcpyAsync(c->pos, pos, 24 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    NB_CUDA(cudaMemcpyAsync(c->mass, mass, 8 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    if (vel) NB_CUDA(cudaMemcpyAsync(c->vel, vel, 24 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    else NB_CUDA(cudaMemsetAsync(c->vel, 0, 24 * (size_t)n, c->stream));
+    c->n = n;
+    c->have_state = true;
+    c->have_vel = vel != nullptr;
+    c->have_acc = false;
+    return NBODY_OK;
+}
+
+int download_acc(nbody_ctx *c, double *acc) {
+    const size_t cnt = 3 * (size_t)c->n;
+    if (c->p.precision == NBODY_PRECISION_FP64) {
+        NB_CUDA(cudaMemcpyAsync(acc, c->acc, 8 * cnt, cudaMemcpyDeviceToHost, c->stream));
+    } else {
+        NB_CUDA(launch_acc_to_double((const float *)c->acc, c->acc_out, cnt, c->stream));
+        c->launches++;
+        NB_CUDA(cudaMemcpyAsync(acc, c->acc_out, 8 * cnt, cudaMemcpyDeviceToHost, c->stream));
+    }
+    return NBODY_OK;
+}
+
+int run_steps(nbody_ctx *c, uint32_t nsteps) {
+    const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
+    StepParams sp{c->p.dt, c->p.adaptive, c->p.min_adaptive_dt, c->p.max_pos_change, c->p.max_vel_change};
+    for (uint32_t s = 0; s < nsteps; s++) {
+        int rc = force_pass(c, c->p.damping, c->p.theta, fp64, c->p.adaptive != 0, c->p.adaptive != 0, false, false);
+        if (rc) return rc;
+        NB_CUDA(launch_update(c->pos, c->vel, c->acc, fp64, c->n, sp, c->sc, c->stream));
+        c->launches++;
+        ev(c, 4);
+    }
+    return NBODY_OK;
+}
+
+#define CTX_OR_FAIL(c)                                                 \
+    do {                                                               \
+        if (!(c)) return fail(NBODY_ERR_INVALID, "context is null%s"); \
+        int rc_ = set_device(c);                                       \
+        if (rc_) return rc_;                                           \
+    } while (0)
+
+}  // namespace
+
+extern "C" {
+
+void nbody_default_params(nbody_params *p) {
+    if (!p) return;
+    p->theta = 0.5;       // src/main.cpp:1327
+    p->dt = 0.0333;       // src/main.cpp:1328
+    p->damping = 0;       // src/main.cpp:1343
+    p->adaptive = 0;      // README.md:54
+    p->min_adaptive_dt = 0.00333;  // README.md:56
+    p->max_pos_change = 3;         // README.md:58
+    p->max_vel_change = 3;         // README.md:60
+    p->precision = NBODY_PRECISION_MIXED;
+    p->device = 0;
+}
+
+int nbody_create(const nbody_params *p, nbody_ctx **out) {
+    if (!out) return fail(NBODY_ERR_INVALID, "out is null%s");
+    *out = nullptr;
+    int rc = check_params(p);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= p->device || p->device < 0) {
+        cudaGetLastError();
+        return fail(NBODY_ERR_NO_DEVICE, "no CUDA device with ordinal %s", "requested");
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, p->device) != cudaSuccess || prop.major != 10) {
+        cudaGetLastError();
+        return fail(NBODY_ERR_NO_DEVICE, "device is not sm_100 (this library is built for sm_100a only)%s");
+    }
+    nbody_ctx *c = new (std::nothrow) nbody_ctx();
+    if (!c) return fail(NBODY_ERR_OOM, "host allocation failed%s");
+    c->p = *p;
+    auto cleanup = [&](int code) { nbody_destroy(c); return code; };
+    if ((rc = set_device(c))) return cleanup(rc);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return cleanup(fail(NBODY_ERR_CUDA, "stream creation failed%s"));
+    c->own_stream = true;
+    if (cudaMalloc(&c->sc, sizeof(DevScalars)) != cudaSuccess) return cleanup(fail(NBODY_ERR_OOM, "scalars%s"));
+    if (cudaMemset(c->sc, 0, sizeof(DevScalars)) != cudaSuccess) return cleanup(fail(NBODY_ERR_CUDA, "memset%s"));
+    if (cudaMallocHost(&c->hsc, sizeof(DevScalars)) != cudaSuccess) return cleanup(fail(NBODY_ERR_OOM, "pinned%s"));
+    std::memset(c->hsc, 0, sizeof(DevScalars));
+    for (auto &e : c->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) return cleanup(fail(NBODY_ERR_CUDA, "event%s"));
+    if (walk_launch_shape(false, p->device, &c->wl_mixed) != cudaSuccess ||
+        walk_launch_shape(true, p->device, &c->wl_fp64) != cudaSuccess)
+        return cleanup(fail(NBODY_ERR_CUDA, "walk kernel configuration failed (%s)",
+                            cudaGetErrorString(cudaGetLastError())));
+    *out = c;
+    return NBODY_OK;
+}
+
+int nbody_destroy(nbody_ctx *c) {
+    if (!c) return NBODY_OK;
+    cudaSetDevice(c->p.device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->arena) cudaFree(c->arena);
+    if (c->sc) cudaFree(c->sc);
+    if (c->hsc) cudaFreeHost(c->hsc);
+    for (auto &e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return NBODY_OK;
+}
+
+int nbody_set_params(nbody_ctx *c, const nbody_params *p) {
+    CTX_OR_FAIL(c);
+    int rc = check_params(p);
+    if (rc) return rc;
+    if (p->device != c->p.device) return fail(NBODY_ERR_INVALID, "device cannot change on a live context%s");
+    if (p->precision != c->p.precision) c->have_acc = false;
+    c->p = *p;
+    return NBODY_OK;
+}
+
+int nbody_set_stream(nbody_ctx *c, void *stream) {
+    CTX_OR_FAIL(c);
+    NB_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    c->stream = (cudaStream_t)stream;
+    c->own_stream = false;
+    return NBODY_OK;
+}
+
+int nbody_set_timing(nbody_ctx *c, int enabled) {
+    CTX_OR_FAIL(c);
+    c->timing = enabled ? 1 : 0;
+    return NBODY_OK;
+}
+
+int nbody_barnes_hut(nbody_ctx *c, uint32_t n, const double *pos, const double *mass, int damping, double theta,
+                     double *acc_out, uint32_t *counts_out) {
+    CTX_OR_FAIL(c);
+    if (n > kMaxParticles) return fail(NBODY_ERR_INVALID, "n exceeds the 2^28 particle limit%s");
+    if (n && (!pos || !mass || !acc_out)) return fail(NBODY_ERR_INVALID, "null array%s");
+    if (!(theta > 0.0) || !std::isfinite(theta)) return fail(NBODY_ERR_INVALID, "theta must be finite and > 0%s");
+    if (n == 0) return NBODY_OK;
+    int rc = upload(c, n, pos, nullptr, mass);
+    if (rc) return rc;
+    if ((rc = begin_call(c))) return rc;
+    const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
+    rc = force_pass(c, damping ? 1 : 0, theta, fp64, false, false, counts_out != nullptr, false);
+    if (rc) return rc;
+    ev(c, 4);
+    if ((rc = download_acc(c, acc_out))) return rc;
+    if (counts_out) NB_CUDA(cudaMemcpyAsync(counts_out, c->counts, 4 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = copy_scalars_back(c))) return rc;
+    return check_status(c);
+}
+
+int nbody_set_particles(nbody_ctx *c, uint32_t n, const double *pos, const double *vel, const double *mass) {
+    CTX_OR_FAIL(c);
+    if (n > kMaxParticles) return fail(NBODY_ERR_INVALID, "n exceeds the 2^28 particle limit%s");
+    if (n && (!pos || !mass)) return fail(NBODY_ERR_INVALID, "null array%s");
+    int rc = upload(c, n, pos, vel, mass);
+    if (rc) return rc;
+    NB_CUDA(cudaStreamSynchronize(c->stream));
+    c->have_vel = true;  // a null vel means zero velocities
+    return NBODY_OK;
+}
+
+int nbody_get_particles(nbody_ctx *c, double *pos, double *vel, double *acc) {
+    CTX_OR_FAIL(c);
+    if (!c->have_state) return fail(NBODY_ERR_STATE, "no particles set%s");
+    if (pos) NB_CUDA(cudaMemcpyAsync(pos, c->pos, 24 * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
+    if (vel) NB_CUDA(cudaMemcpyAsync(vel, c->vel, 24 * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
+    if (acc) {
+        if (!c->have_acc) return fail(NBODY_ERR_STATE, "no forces computed yet%s");
+        int rc = download_acc(c, acc);
+        if (rc) return rc;
+    }
+    NB_CUDA(cudaStreamSynchronize(c->stream));
+    return NBODY_OK;
+}
+
+int nbody_compute_forces(nbody_ctx *c) {
+    CTX_OR_FAIL(c);
+    if (!c->have_state) return fail(NBODY_ERR_STATE, "no particles set%s");
+    if (c->n == 0) return NBODY_OK;
+    int rc = begin_call(c);
+    if (rc) return rc;
+    rc = force_pass(c, c->p.damping, c->p.theta, c->p.precision == NBODY_PRECISION_FP64, false, false, false, false);
+    if (rc) return rc;
+    ev(c, 4);
+    if ((rc = copy_scalars_back(c))) return rc;
+    return check_status(c);
+}
+
+int nbody_step(nbody_ctx *c, uint32_t nsteps) {
+    CTX_OR_FAIL(c);
+    if (!c->have_state || !c->have_vel) return fail(NBODY_ERR_STATE, "particles with velocities must be set first%s");
+    if (c->n == 0 || nsteps == 0) return NBODY_OK;
+    int rc = begin_call(c);
+    if (rc) return rc;
+    rc = run_steps(c, nsteps);
+    if (rc) return rc;
+    if ((rc = copy_scalars_back(c))) return rc;
+    return check_status(c);
+}
+
+int nbody_step_host(nbody_ctx *c, uint32_t n, double *pos, double *vel, const double *mass, uint32_t nsteps) {
+    CTX_OR_FAIL(c);
+    if (n > kMaxParticles) return fail(NBODY_ERR_INVALID, "n exceeds the 2^28 particle limit%s");
+    if (n && (!pos || !vel || !mass)) return fail(NBODY_ERR_INVALID, "null array%s");
+    if (n == 0) return NBODY_OK;
+    int rc = upload(c, n, pos, vel, mass);
+    if (rc) return rc;
+    c->have_vel = true;
+    if ((rc = begin_call(c))) return rc;
+    if ((rc = run_steps(c, nsteps))) return rc;
+    NB_CUDA(cudaMemcpyAsync(pos, c->pos, 24 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    NB_CUDA(cudaMemcpyAsync(vel, c->vel, 24 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = copy_scalars_back(c))) return rc;
+    return check_status(c);
+}
+
+int nbody_device_view_get(nbody_ctx *c, nbody_device_view *out) {
+    CTX_OR_FAIL(c);
+    if (!out) return fail(NBODY_ERR_INVALID, "out is null%s");
+    if (!c->have_state) return fail(NBODY_ERR_STATE, "no particles set%s");
+    out->n = c->n;
+    out->pos = c->pos;
+    out->vel = c->vel;
+    out->mass = c->mass;
+    out->acc = c->acc;
+    out->acc_is_double = c->p.precision == NBODY_PRECISION_FP64;
+    return NBODY_OK;
+}
+
+int nbody_get_stats(nbody_ctx *c, nbody_stats *out) {
+    if (!c || !out) return fail(NBODY_ERR_INVALID, "null argument%s");
+    *out = c->stats;
+    return NBODY_OK;
+}
+
+int nbody_get_diagnostics(nbody_ctx *c, nbody_diagnostics *out) {
+    CTX_OR_FAIL(c);
+    if (!out) return fail(NBODY_ERR_INVALID, "out is null%s");
+    if (!c->have_state) return fail(NBODY_ERR_STATE, "no particles set%s");
+    std::memset(out, 0, sizeof *out);
+    if (c->n == 0) return NBODY_OK;
+    const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
+    int rc = begin_call(c);
+    if (rc) return rc;
+    rc = force_pass(c, c->p.damping, c->p.theta, fp64, false, false, false, true);
+    if (rc) return rc;
+    ev(c, 4);
+    NB_CUDA(launch_diag(c->pos, c->vel, c->mass, c->pot, c->n, c->diag_partial, kDiagBlocks, c->sc, c->stream));
+    c->launches++;
+    if ((rc = copy_scalars_back(c))) return rc;
+    if ((rc = check_status(c))) return rc;
+    const double *d = c->hsc->diag;
+    out->kinetic = d[0];
+    out->potential = d[1];
+    for (int k = 0; k < 3; k++) {
+        out->momentum[k] = d[2 + k];
+        out->angular_momentum[k] = d[5 + k];
+        out->com[k] = d[8] != 0.0 ? d[9 + k] / d[8] : 0.0;
+    }
+    out->mass = d[8];
+    return NBODY_OK;
+}
+
+const char *nbody_status_string(int s) {
+    switch (s) {
+        case NBODY_OK: return "ok";
+        case NBODY_ERR_INVALID: return "invalid argument";
+        case NBODY_ERR_CUDA: return "CUDA error";
+        case NBODY_ERR_OOM: return "out of memory";
+        case NBODY_ERR_COINCIDENT: return "coincident particles";
+        case NBODY_ERR_NONFINITE: return "non-finite position or mass";
+        case NBODY_ERR_CAPACITY: return "walk stack capacity exceeded";
+        case NBODY_ERR_NO_DEVICE: return "no sm_100 CUDA device";
+        case NBODY_ERR_STATE: return "call out of order";
+        default: return "unknown status";
+    }
+}
+
+const char *nbody_last_error_message(void) { return g_msg; }
+
+}  // extern "C"

@@ -1,0 +1,87 @@
+// Shared definitions of the nbody_b200 kernels (sm_100a).
+//
+// Data layout in HBM (capacity `cap` particles, grown on demand, never freed
+// per step):
+//   user order    pos, vel  : double[3*cap] (AoS, the host layout)
+//                 mass      : double[cap]
+//                 acc       : float[3*cap] (MIXED) or double[3*cap] (FP64)
+//   sort          key1/idx  : u64/u32 [cap] x2 (ping-pong), key2/key3 u64[cap] (deep keys)
+//   sorted bodies body      : double4[cap] = (x, y, z, m) in Morton order
+//   binary tree   bleft/bright/bparent : i32[cap], bdelta u8..i32[cap], leaf_bparent i32[cap]
+//   octree        onode     : double4[cap] = (com.x, com.y, com.z, mass)
+//                 ochild    : i32[8*cap]  (>= 0 internal node, < 0 leaf ~sorted index)
+//                 ometa     : i32[cap]    level | nchild << 8
+//                 oparent   : i32[cap], leaf_oparent : i32[cap], ocount : u32[cap]
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace nbody {
+
+constexpr double kG = 6.67384e-11;  // src/main.cpp:322
+constexpr int kLevelsPerWord = 21;  // 63 key bits per 64-bit word, 3 bits per octree level
+constexpr int kMaxWords = 3;        // up to 63 levels below the root cube
+constexpr int kMaxLevels = kLevelsPerWord * kMaxWords;
+
+// Device status bits (OR-ed by kernels, read by the host after a pass).
+enum : uint32_t {
+    kStatusNonFinite = 1u << 0,
+    kStatusCoincident = 1u << 1,
+    kStatusCapacity = 1u << 2,
+    kStatusDeepGroup = 1u << 3,  // a group of equal 21-level keys needed deep keys
+};
+
+struct DevScalars {
+    double root_center[3];
+    double root_side;
+    double bbox_min[3];
+    double bbox_max[3];
+    unsigned long long interactions;
+    unsigned long long interactions_total;  // summed over the steps of one API call
+    uint32_t status;
+    uint32_t n_onodes;
+    uint32_t depth;
+    uint32_t max_stack;
+    uint32_t fallback_tests;
+    uint32_t group_counter;
+    uint32_t ticket;          // last-block tickets of reductions
+    uint32_t deep_groups;
+    unsigned long long max_acc_bits;  // max |a| (non-negative double as ordered bits)
+    unsigned long long max_vel_bits;  // max |v|
+    double dt_used;
+    double diag[16];          // kinetic, potential, momentum[3], L[3], mass, m*x[3]
+};
+
+struct Tree {
+    uint32_t n;
+    const double4 *body;       // sorted (x, y, z, m)
+    const uint32_t *sidx;      // sorted position -> user index
+    const double4 *onode;      // internal nodes (com, mass)
+    const int32_t *ochild;     // 8 per node
+    const int32_t *ometa;      // level | nchild << 8
+    DevScalars *sc;
+};
+
+__host__ __device__ inline int meta_level(int32_t m) { return m & 0xff; }
+__host__ __device__ inline int meta_nchild(int32_t m) { return (m >> 8) & 0xf; }
+
+// Non-negative doubles compare like their bit patterns.
+__device__ inline void atomic_max_nonneg(unsigned long long *a, double v) {
+    atomicMax(a, (unsigned long long)__double_as_longlong(v));
+}
+
+__device__ inline double warp_min(double v) {
+    for (int o = 16; o; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ inline double warp_max(double v) {
+    for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ inline double warp_sum(double v) {
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+}  // namespace nbody

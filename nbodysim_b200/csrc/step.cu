@@ -1,0 +1,137 @@
+// Integration step, adaptive dt and FP64 diagnostics.
+#include "step.cuh"
+
+namespace nbody {
+
+// Semi-implicit Euler exactly as particle::update (src/particle.cpp:66-74):
+// v = v + (a dt); x = x + (v dt), each product and sum rounded on its own.
+// Adaptive dt (README.md:54-60 names the keys; the reference has no code):
+//   dt_k = clamp(min(dt, max_vel_change / max|a|, max_pos_change / max|v|),
+//                min_adaptive_dt, dt)
+// with clamp as src/main.cpp:177-182 defines it and |v| taken before the kick.
+template <typename AccT>
+__global__ void k_update(double *__restrict__ pos, double *__restrict__ vel, const AccT *__restrict__ acc,
+                         uint32_t n, StepParams sp, DevScalars *sc) {
+    double dt = sp.dt;
+    if (sp.adaptive) {
+        const double amax = __longlong_as_double((long long)sc->max_acc_bits);
+        const double vmax = __longlong_as_double((long long)sc->max_vel_bits);
+        double c = sp.dt;
+        if (amax > 0.0) c = fmin(c, sp.max_vel_change / amax);
+        if (vmax > 0.0) c = fmin(c, sp.max_pos_change / vmax);
+        if (c < sp.min_adaptive_dt) c = sp.min_adaptive_dt;
+        else if (c > sp.dt) c = sp.dt;
+        dt = c;
+    }
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) sc->dt_used = dt;
+    if (i >= n) return;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const size_t o = 3 * (size_t)i + k;
+        const double v = __dadd_rn(vel[o], __dmul_rn((double)acc[o], dt));
+        vel[o] = v;
+        pos[o] = __dadd_rn(pos[o], __dmul_rn(v, dt));
+    }
+}
+
+// FP64 sums: kinetic, potential (1/2 sum m phi), momentum, angular momentum,
+// mass, mass-weighted position. Block partials, then the last block sums the
+// partials in block order, so the result does not depend on scheduling.
+__global__ void k_diag(const double *__restrict__ pos, const double *__restrict__ vel,
+                       const double *__restrict__ mass, const double *__restrict__ pot, uint32_t n,
+                       double *__restrict__ partial, DevScalars *sc) {
+    constexpr int K = kDiagCount;
+    __shared__ double s_red[K][32];
+    __shared__ bool s_last;
+    double v[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double m = mass[i];
+        const double x = pos[3 * (size_t)i], y = pos[3 * (size_t)i + 1], z = pos[3 * (size_t)i + 2];
+        const double vx = vel[3 * (size_t)i], vy = vel[3 * (size_t)i + 1], vz = vel[3 * (size_t)i + 2];
+        v[0] += 0.5 * m * (vx * vx + vy * vy + vz * vz);
+        v[1] += pot ? 0.5 * m * pot[i] : 0.0;
+        v[2] += m * vx; v[3] += m * vy; v[4] += m * vz;
+        v[5] += m * (y * vz - z * vy);
+        v[6] += m * (z * vx - x * vz);
+        v[7] += m * (x * vy - y * vx);
+        v[8] += m;
+        v[9] += m * x; v[10] += m * y; v[11] += m * z;
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        double r = warp_sum(v[k]);
+        if (lane == 0) s_red[k][wid] = r;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        for (int k = 0; k < K; k++) {
+            double r = lane < nw ? s_red[k][lane] : 0.0;
+            r = warp_sum(r);
+            if (lane == 0) partial[K * blockIdx.x + k] = r;
+        }
+        if (lane == 0) {
+            __threadfence();
+            s_last = atomicAdd(&sc->ticket, 1u) == gridDim.x - 1;
+        }
+    }
+    __syncthreads();
+    if (!s_last || threadIdx.x != 0) return;
+    __threadfence();
+    for (int k = 0; k < K; k++) {
+        double acc = 0.0;
+        for (uint32_t b = 0; b < gridDim.x; b++) acc += __ldcg(&partial[K * b + k]);
+        sc->diag[k] = acc;
+    }
+    sc->ticket = 0;
+}
+
+__global__ void k_reset_pass(DevScalars *sc) {
+    sc->interactions = 0;
+    sc->n_onodes = 0;
+    sc->depth = 0;
+    sc->max_stack = 0;
+    sc->fallback_tests = 0;
+    sc->group_counter = 0;
+    sc->ticket = 0;
+    sc->deep_groups = 0;
+    sc->max_acc_bits = 0;
+    sc->max_vel_bits = 0;
+}
+
+__global__ void k_acc_to_double(const float *__restrict__ in, double *__restrict__ out, size_t count) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) out[i] = (double)in[i];
+}
+
+cudaError_t launch_update(double *pos, double *vel, const void *acc, bool acc_double, uint32_t n,
+                          const StepParams &sp, DevScalars *sc, cudaStream_t st) {
+    const unsigned blocks = n ? (n + 255) / 256 : 1;
+    if (acc_double)
+        k_update<double><<<blocks, 256, 0, st>>>(pos, vel, (const double *)acc, n, sp, sc);
+    else
+        k_update<float><<<blocks, 256, 0, st>>>(pos, vel, (const float *)acc, n, sp, sc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_diag(const double *pos, const double *vel, const double *mass, const double *pot,
+                        uint32_t n, double *partial, unsigned blocks, DevScalars *sc, cudaStream_t st) {
+    k_diag<<<blocks, 256, 0, st>>>(pos, vel, mass, pot, n, partial, sc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reset_pass(DevScalars *sc, cudaStream_t st) {
+    k_reset_pass<<<1, 1, 0, st>>>(sc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_acc_to_double(const float *in, double *out, size_t count, cudaStream_t st) {
+    if (!count) return cudaSuccess;
+    k_acc_to_double<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(in, out, count);
+    return cudaGetLastError();
+}
+
+}  // namespace nbody

@@ -1,0 +1,574 @@
+// Octree construction on the GPU: root cube, Morton-order keys, radix sort,
+// binary radix tree, chain-free octree, bottom-up mass / centre of mass.
+//
+// The tree is the reference's octree (src/octree.cpp:54-196, src/main.cpp:887-927)
+// with single-child chains collapsed: a node exists here iff the reference
+// node at the same cell has two or more non-empty children (or is the root's
+// first branching descendant). Chains carry the same mass and, up to rounding
+// emulated below, the same centre of mass as their bottom node, so every
+// particle's walk accepts the same bodies (see walk.cu).
+#include "tree.cuh"
+
+#include <cstdio>
+
+namespace nbody {
+
+// ---------------------------------------------------------------------------
+// Root cube: bbox midpoint; side = largest extent + 2.0, a tie for the largest
+// extent falls through to the z extent (src/main.cpp:898-920). Also flags
+// non-finite positions or masses, and (optionally) reduces max |v| for the
+// adaptive step.
+__global__ void k_bbox(const double *__restrict__ pos, const double *__restrict__ vel,
+                       const double *__restrict__ mass, uint32_t n, double *__restrict__ partial,
+                       DevScalars *sc) {
+    __shared__ double s_red[7][32];
+    __shared__ bool s_last;
+    double mn[3] = {INFINITY, INFINITY, INFINITY};
+    double mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    double vmax = 0.0;
+    bool bad = false;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double x = pos[3 * (size_t)i], y = pos[3 * (size_t)i + 1], z = pos[3 * (size_t)i + 2];
+        double m = mass[i];
+        bad |= !(isfinite(x) && isfinite(y) && isfinite(z) && isfinite(m));
+        mn[0] = fmin(mn[0], x); mx[0] = fmax(mx[0], x);
+        mn[1] = fmin(mn[1], y); mx[1] = fmax(mx[1], y);
+        mn[2] = fmin(mn[2], z); mx[2] = fmax(mx[2], z);
+        if (vel) {
+            double vx = vel[3 * (size_t)i], vy = vel[3 * (size_t)i + 1], vz = vel[3 * (size_t)i + 2];
+            vmax = fmax(vmax, sqrt(vx * vx + vy * vy + vz * vz));
+        }
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&sc->status, kStatusNonFinite);
+    double v[7] = {mn[0], mn[1], mn[2], -mx[0], -mx[1], -mx[2], -vmax};
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int k = 0; k < 7; k++) {
+        double r = warp_min(v[k]);
+        if (lane == 0) s_red[k][wid] = r;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        for (int k = 0; k < 7; k++) {
+            double r = lane < nw ? s_red[k][lane] : INFINITY;
+            r = warp_min(r);
+            if (lane == 0) partial[7 * blockIdx.x + k] = r;
+        }
+        if (lane == 0) {
+            __threadfence();
+            s_last = atomicAdd(&sc->ticket, 1u) == gridDim.x - 1;
+        }
+    }
+    __syncthreads();
+    if (!s_last || wid != 0) return;
+    __threadfence();
+    double r[7];
+    for (int k = 0; k < 7; k++) {
+        double acc = INFINITY;
+        for (uint32_t b = lane; b < gridDim.x; b += 32) acc = fmin(acc, __ldcg(&partial[7 * b + k]));
+        r[k] = warp_min(acc);
+    }
+    if (lane == 0) {
+        double lo[3] = {r[0], r[1], r[2]}, hi[3] = {-r[3], -r[4], -r[5]};
+        for (int k = 0; k < 3; k++) {
+            sc->bbox_min[k] = lo[k];
+            sc->bbox_max[k] = hi[k];
+            sc->root_center[k] = (lo[k] + hi[k]) / 2.0;
+        }
+        double ex = hi[0] - lo[0], ey = hi[1] - lo[1], ez = hi[2] - lo[2];
+        double side;
+        if (ex > ey && ex > ez) side = ex + 2.0;
+        else if (ey > ex && ey > ez) side = ey + 2.0;
+        else side = ez + 2.0;
+        sc->root_side = side;
+        sc->max_vel_bits = (unsigned long long)__double_as_longlong(-r[6]);
+        sc->ticket = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Octant digits by descent from the root cube, rounding every child centre
+// exactly as allocate_child does (src/octree.cpp:65-84: center + (+-1 * half) / 2
+// with half = side / 2), and choosing the octant with strict '>' as
+// add_particle does (src/octree.cpp:153-165). Digits are (z<<2)|(y<<1)|x so
+// that Morton order equals the reference's child order 0..7.
+__device__ inline uint64_t descend_word(double x, double y, double z, double &cx, double &cy,
+                                        double &cz, double &side) {
+    uint64_t key = 0;
+#pragma unroll 3
+    for (int l = 0; l < kLevelsPerWord; l++) {
+        double half = side / 2;
+        double q = half / 2;
+        int bx = x > cx, by = y > cy, bz = z > cz;
+        key = (key << 3) | (uint64_t)((bz << 2) | (by << 1) | bx);
+        cx = __dadd_rn(cx, bx ? q : -q);
+        cy = __dadd_rn(cy, by ? q : -q);
+        cz = __dadd_rn(cz, bz ? q : -q);
+        side = half;
+    }
+    return key;
+}
+
+__global__ void k_keys(const double *__restrict__ pos, uint32_t n, const DevScalars *sc,
+                       uint64_t *__restrict__ key, uint32_t *__restrict__ idx) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double cx = sc->root_center[0], cy = sc->root_center[1], cz = sc->root_center[2];
+    double side = sc->root_side;
+    key[i] = descend_word(pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2], cx, cy,
+                          cz, side);
+    idx[i] = i;
+}
+
+// ---------------------------------------------------------------------------
+// LSD radix sort of (key, idx), 8-bit digits, stable per pass:
+// histogram per tile -> exclusive scan (digit-major) -> ranked scatter.
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;
+
+__global__ void k_sort_hist(const uint64_t *__restrict__ key, uint32_t n, int shift,
+                            uint32_t *__restrict__ hist, uint32_t nblocks) {
+    __shared__ uint32_t s_h[256];
+    s_h[threadIdx.x] = 0;
+    __syncthreads();
+    uint32_t base = blockIdx.x * kSortTile;
+    for (int r = 0; r < kSortItems; r++) {
+        uint32_t i = base + r * kSortThreads + threadIdx.x;
+        if (i < n) atomicAdd(&s_h[(key[i] >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    hist[threadIdx.x * nblocks + blockIdx.x] = s_h[threadIdx.x];
+}
+
+// Exclusive prefix sum of u32 values in place: tiles of 4096 scanned per
+// block, tile totals scanned by one block, then added back.
+constexpr int kScanThreads = 1024;
+constexpr int kScanTile = 4 * kScanThreads;
+
+__device__ inline uint32_t block_exclusive_scan(uint32_t x, uint32_t *s_warp, uint32_t *total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t incl = x;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t w = lane < (int)(blockDim.x >> 5) ? s_warp[lane] : 0;
+        uint32_t wi = w;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += y;
+        }
+        s_warp[lane] = wi - w;
+        if (lane == 31) s_warp[32] = wi;
+    }
+    __syncthreads();
+    uint32_t r = s_warp[wid] + incl - x;
+    if (total) *total = s_warp[32];
+    return r;
+}
+
+__global__ void k_scan_tiles(uint32_t *__restrict__ v, uint32_t len, uint32_t *__restrict__ tile_sums) {
+    __shared__ uint32_t s_warp[33];
+    const uint32_t base = blockIdx.x * kScanTile + 4 * threadIdx.x;
+    uint32_t x[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) x[k] = base + k < len ? v[base + k] : 0u;
+    uint32_t s = x[0] + x[1] + x[2] + x[3];
+    uint32_t tot;
+    uint32_t run = block_exclusive_scan(s, s_warp, &tot);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        if (base + k < len) v[base + k] = run;
+        run += x[k];
+    }
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+}
+
+// One block: exclusive scan of up to a few thousand tile totals; writes the grand total.
+__global__ void k_scan_small(uint32_t *__restrict__ v, uint32_t len, uint32_t *total) {
+    __shared__ uint32_t s_warp[33];
+    uint32_t carry = 0;
+    for (uint32_t b = 0; b < len; b += blockDim.x) {
+        uint32_t i = b + threadIdx.x;
+        uint32_t x = i < len ? v[i] : 0u;
+        uint32_t tot;
+        uint32_t r = block_exclusive_scan(x, s_warp, &tot);
+        if (i < len) v[i] = r + carry;
+        carry += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && total) *total = carry;
+}
+
+__global__ void k_scan_add(uint32_t *__restrict__ v, uint32_t len, const uint32_t *__restrict__ tile_sums) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < len) v[i] += tile_sums[i / kScanTile];
+}
+
+unsigned scan_exclusive(uint32_t *v, uint32_t len, uint32_t *tile_sums, uint32_t *total, cudaStream_t st) {
+    const uint32_t tiles = (len + kScanTile - 1) / kScanTile;
+    k_scan_tiles<<<tiles, kScanThreads, 0, st>>>(v, len, tile_sums);
+    k_scan_small<<<1, kScanThreads, 0, st>>>(tile_sums, tiles, total);
+    if (tiles > 1) k_scan_add<<<(len + 255) / 256, 256, 0, st>>>(v, len, tile_sums);
+    return tiles > 1 ? 3u : 2u;
+}
+
+__global__ void k_sort_scatter(const uint64_t *__restrict__ key_in, const uint32_t *__restrict__ idx_in,
+                               uint64_t *__restrict__ key_out, uint32_t *__restrict__ idx_out,
+                               uint32_t n, int shift, const uint32_t *__restrict__ hist,
+                               uint32_t nblocks) {
+    __shared__ uint32_t s_off[256];
+    __shared__ uint32_t s_w[kSortThreads / 32][256];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    s_off[t] = hist[t * nblocks + blockIdx.x];
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t base = blockIdx.x * kSortTile;
+    for (int r = 0; r < kSortItems; r++) {
+#pragma unroll
+        for (int w = 0; w < kSortThreads / 32; w++) s_w[w][t] = 0;
+        __syncthreads();
+        uint32_t i = base + r * kSortThreads + t;
+        bool valid = i < n;
+        uint64_t k = valid ? key_in[i] : 0;
+        uint32_t v = valid ? idx_in[i] : 0;
+        uint32_t d = (uint32_t)((k >> shift) & 255u);
+        uint32_t tag = valid ? d : (256u + lane);
+        uint32_t peers = __match_any_sync(0xffffffffu, tag);
+        uint32_t rank = __popc(peers & lt);
+        if (valid && rank == 0) s_w[warp][d] = __popc(peers);
+        __syncthreads();
+        {
+            uint32_t run = s_off[t];
+#pragma unroll
+            for (int w = 0; w < kSortThreads / 32; w++) {
+                uint32_t c = s_w[w][t];
+                s_w[w][t] = run;
+                run += c;
+            }
+            s_off[t] = run;
+        }
+        __syncthreads();
+        if (valid) {
+            uint32_t p = s_w[warp][d] + rank;
+            key_out[p] = k;
+            idx_out[p] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+__global__ void k_gather_bodies(const uint32_t *__restrict__ idx, const double *__restrict__ pos,
+                                const double *__restrict__ mass, double4 *__restrict__ body,
+                                uint32_t n) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    uint32_t i = idx[j];
+    body[j] = make_double4(pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2], mass[i]);
+}
+
+// Groups of particles whose 21-level keys agree get two more key words
+// (levels 22..63) and are re-sorted among themselves. Identical keys over all
+// 63 levels mean coincident particles (the reference recurses without bound).
+constexpr int kMaxDeepGroup = 64;
+
+__global__ void k_deep_groups(uint64_t *__restrict__ key1, uint64_t *__restrict__ key2,
+                              uint64_t *__restrict__ key3, uint32_t *__restrict__ idx,
+                              double4 *__restrict__ body, uint32_t n, DevScalars *sc) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i + 1 >= n) return;
+    uint64_t k = key1[i];
+    if (key1[i + 1] != k) return;
+    if (i > 0 && key1[i - 1] == k) return;  // not the first of its group
+    uint32_t e = i + 1;
+    while (e + 1 < n && key1[e + 1] == k) e++;
+    uint32_t g = e - i + 1;
+    atomicAdd(&sc->deep_groups, 1u);
+    atomicOr(&sc->status, kStatusDeepGroup);
+    if (g > kMaxDeepGroup) {
+        // Too many particles in one cell of side 2^-21 of the root: reported as
+        // coincident. Zero deep keys keep the radix tree well formed (ties
+        // then break on sorted position).
+        for (uint32_t j = i; j <= e; j++) key2[j] = key3[j] = 0;
+        atomicOr(&sc->status, kStatusCoincident);
+        return;
+    }
+    const double rcx = sc->root_center[0], rcy = sc->root_center[1], rcz = sc->root_center[2];
+    const double rs = sc->root_side;
+    for (uint32_t j = i; j <= e; j++) {
+        double4 b = body[j];
+        double cx = rcx, cy = rcy, cz = rcz, s = rs;
+        descend_word(b.x, b.y, b.z, cx, cy, cz, s);
+        key2[j] = descend_word(b.x, b.y, b.z, cx, cy, cz, s);
+        key3[j] = descend_word(b.x, b.y, b.z, cx, cy, cz, s);
+    }
+    // insertion sort of the group by (key2, key3)
+    for (uint32_t j = i + 1; j <= e; j++) {
+        uint64_t a2 = key2[j], a3 = key3[j];
+        uint32_t ai = idx[j];
+        double4 ab = body[j];
+        uint32_t p = j;
+        while (p > i && (key2[p - 1] > a2 || (key2[p - 1] == a2 && key3[p - 1] > a3))) {
+            key2[p] = key2[p - 1]; key3[p] = key3[p - 1]; idx[p] = idx[p - 1]; body[p] = body[p - 1];
+            p--;
+        }
+        key2[p] = a2; key3[p] = a3; idx[p] = ai; body[p] = ab;
+    }
+    for (uint32_t j = i; j < e; j++)
+        if (key2[j] == key2[j + 1] && key3[j] == key3[j + 1]) atomicOr(&sc->status, kStatusCoincident);
+}
+
+// ---------------------------------------------------------------------------
+// Binary radix tree (Karras 2012, "Maximizing parallelism in the construction
+// of BVHs, octrees and k-d trees"), prefix lengths in key bits over up to
+// three 63-bit words; exact duplicates fall back to index bits so the tree
+// stays well formed while the coincident status reports the error.
+struct KeyView {
+    const uint64_t *k1, *k2, *k3;
+    int n;
+    __device__ int delta(int i, int j) const {
+        if (j < 0 || j >= n) return -1;
+        uint64_t a = k1[i], b = k1[j];
+        if (a != b) return __clzll(a ^ b) - 1;
+        a = k2[i]; b = k2[j];
+        if (a != b) return 63 + __clzll(a ^ b) - 1;
+        a = k3[i]; b = k3[j];
+        if (a != b) return 126 + __clzll(a ^ b) - 1;
+        return 189 + __clz((unsigned)i ^ (unsigned)j);
+    }
+};
+
+__device__ inline int level_of(int delta) { return min(delta / 3, kMaxLevels); }
+
+__global__ void k_radix_tree(KeyView kv, int32_t *__restrict__ bleft, int32_t *__restrict__ bright,
+                             int32_t *__restrict__ bparent, int32_t *__restrict__ leaf_bparent,
+                             int32_t *__restrict__ bdelta) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = kv.n;
+    if (i >= n - 1) return;
+    int d = (kv.delta(i, i + 1) - kv.delta(i, i - 1)) >= 0 ? 1 : -1;
+    int dmin = kv.delta(i, i - d);
+    int lmax = 2;
+    while (kv.delta(i, i + lmax * d) > dmin) lmax <<= 1;
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+        if (kv.delta(i, i + (l + t) * d) > dmin) l += t;
+    int j = i + l * d;
+    int dnode = kv.delta(i, j);
+    int s = 0, t = l;
+    do {
+        t = (t + 1) >> 1;
+        if (kv.delta(i, i + (s + t) * d) > dnode) s += t;
+    } while (t > 1);
+    int gamma = i + s * d + min(d, 0);
+    int lo = min(i, j), hi = max(i, j);
+    // children encoded: >= 0 internal binary node, < 0 leaf ~index
+    int left = (lo == gamma) ? ~gamma : gamma;
+    int right = (hi == gamma + 1) ? ~(gamma + 1) : gamma + 1;
+    bleft[i] = left;
+    bright[i] = right;
+    bdelta[i] = dnode;
+    if (left >= 0) bparent[left] = i; else leaf_bparent[~left] = i;
+    if (right >= 0) bparent[right] = i; else leaf_bparent[~right] = i;
+    if (i == 0) bparent[0] = -1;
+}
+
+// A binary node heads an octree node iff it is the root or its parent sits
+// at a shallower octree level.
+__global__ void k_head_flags(const int32_t *__restrict__ bparent, const int32_t *__restrict__ bdelta,
+                             uint32_t m, uint32_t *__restrict__ flag) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    int p = bparent[i];
+    flag[i] = (i == 0 || level_of(bdelta[p]) < level_of(bdelta[i])) ? 1u : 0u;
+}
+
+// Each head gathers, left to right, the exits of its same-level binary
+// subtree: leaves and deeper heads. Left-to-right is Morton order, i.e. the
+// reference's child order 0..7.
+__global__ void k_collapse(const int32_t *__restrict__ bleft, const int32_t *__restrict__ bright,
+                           const int32_t *__restrict__ bdelta, const uint32_t *__restrict__ head_id,
+                           const uint32_t *__restrict__ flag, uint32_t m, int32_t *__restrict__ ochild,
+                           int32_t *__restrict__ ometa, int32_t *__restrict__ oparent,
+                           int32_t *__restrict__ leaf_oparent, DevScalars *sc) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m || !flag[i]) return;
+    const int id = (int)head_id[i];
+    const int L = level_of(bdelta[i]);
+    // In-order walk over the same-level binary nodes (at most 7 of them):
+    // a frame visits its left child, then its right child.
+    int fnode[8], fstate[8];
+    int fs = 0, nch = 0;
+    fnode[0] = (int)i; fstate[0] = 0; fs = 1;
+    while (fs > 0) {
+        const int x = fnode[fs - 1];
+        if (fstate[fs - 1] == 2) { fs--; continue; }
+        const int ch = fstate[fs - 1] == 0 ? bleft[x] : bright[x];
+        fstate[fs - 1]++;
+        if (ch >= 0 && level_of(bdelta[ch]) == L) {
+            if (fs < 8) { fnode[fs] = ch; fstate[fs] = 0; fs++; }
+            else atomicOr(&sc->status, kStatusCapacity);
+        } else if (nch < 8) {
+            if (ch < 0) {
+                ochild[8 * id + nch] = ch;
+                leaf_oparent[~ch] = id;
+            } else {
+                const int cid = (int)head_id[ch];
+                ochild[8 * id + nch] = cid;
+                oparent[cid] = id;
+            }
+            nch++;
+        } else {
+            atomicOr(&sc->status, kStatusCapacity);
+        }
+    }
+    ometa[id] = L | (min(nch, 8) << 8);
+    if (id == 0) oparent[0] = -1;
+    atomicMax(&sc->depth, (uint32_t)L);
+}
+
+// ---------------------------------------------------------------------------
+// Bottom-up mass and centre of mass (src/octree.cpp:203-221, 252-278): one
+// thread per leaf climbs while it is the last child to finish. Sums run in
+// child order with explicit round-to-nearest operations (no FMA contraction),
+// as the reference computes them. A child separated from its parent by k
+// single-child chain nodes enters with its centre of mass passed k times
+// through the chain's (c * m) / m, the value the reference's chain top holds.
+__device__ inline double3 load_node_com(const double4 *p, double &m) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    double2 a = __ldcg(q), b = __ldcg(q + 1);
+    m = b.y;
+    return make_double3(a.x, a.y, b.x);
+}
+
+__global__ void k_com(const double4 *__restrict__ body, const int32_t *__restrict__ leaf_oparent,
+                      const int32_t *__restrict__ oparent, const int32_t *__restrict__ ochild,
+                      const int32_t *__restrict__ ometa, double4 *onode, uint32_t *ocount,
+                      uint32_t n, DevScalars *sc) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    int p = leaf_oparent[j];
+    // A well-formed tree is at most kMaxLevels + 1 internal levels deep; the
+    // bound only guards against a malformed tree after a reported error.
+    for (int hops = 0; p >= 0; hops++) {
+        if (hops > kMaxLevels + 1 || p >= (int)(n - 1)) {
+            atomicOr(&sc->status, kStatusCapacity);
+            return;
+        }
+        const int32_t meta = ometa[p];
+        const int nch = meta_nchild(meta);
+        __threadfence();
+        uint32_t old = atomicAdd(&ocount[p], 1u);
+        if (old != (uint32_t)(nch - 1)) return;
+        __threadfence();
+        const int L = meta_level(meta);
+        double cm[8];
+        double3 cc[8];
+        double m = 0.0;
+        for (int k = 0; k < nch; k++) {
+            int c = ochild[8 * p + k];
+            if (c < 0) {
+                double4 b = body[~c];
+                cm[k] = b.w;
+                cc[k] = make_double3(b.x, b.y, b.z);
+            } else {
+                cc[k] = load_node_com(&onode[c], cm[k]);
+                int chain = meta_level(ometa[c]) - L - 1;
+                for (int t = 0; t < chain; t++) {
+                    if (cm[k] == 0.0) {
+                        cc[k] = make_double3(0.0, 0.0, 0.0);
+                    } else {
+                        cc[k].x = __ddiv_rn(__dmul_rn(cc[k].x, cm[k]), cm[k]);
+                        cc[k].y = __ddiv_rn(__dmul_rn(cc[k].y, cm[k]), cm[k]);
+                        cc[k].z = __ddiv_rn(__dmul_rn(cc[k].z, cm[k]), cm[k]);
+                    }
+                }
+            }
+            m = __dadd_rn(m, cm[k]);
+        }
+        double4 out;
+        out.w = m;
+        if (m == 0.0) {
+            out.x = out.y = out.z = 0.0;
+        } else {
+            double sx = 0.0, sy = 0.0, sz = 0.0;
+            for (int k = 0; k < nch; k++) {
+                sx = __dadd_rn(sx, __dmul_rn(cc[k].x, cm[k]));
+                sy = __dadd_rn(sy, __dmul_rn(cc[k].y, cm[k]));
+                sz = __dadd_rn(sz, __dmul_rn(cc[k].z, cm[k]));
+            }
+            out.x = __ddiv_rn(sx, m);
+            out.y = __ddiv_rn(sy, m);
+            out.z = __ddiv_rn(sz, m);
+        }
+        double2 *q = reinterpret_cast<double2 *>(&onode[p]);
+        __stcg(q, make_double2(out.x, out.y));
+        __stcg(q + 1, make_double2(out.z, out.w));
+        p = oparent[p];
+    }
+}
+
+// ---------------------------------------------------------------------------
+static inline unsigned blocks_for(uint64_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launches) {
+    const uint32_t n = tb.n;
+    unsigned L = 0;
+    if (n == 0) return cudaSuccess;
+    // root cube (+ max |v| when requested)
+    k_bbox<<<tb.bbox_blocks, 256, 0, st>>>(tb.pos, tb.vel_for_max, tb.mass, n, tb.bbox_partial, tb.sc);
+    k_keys<<<blocks_for(n, 256), 256, 0, st>>>(tb.pos, n, tb.sc, tb.key_a, tb.idx_a);
+    L += 2;
+    // radix sort over the 63 key bits
+    uint64_t *kin = tb.key_a, *kout = tb.key_b;
+    uint32_t *iin = tb.idx_a, *iout = tb.idx_b;
+    const uint32_t nb = blocks_for(n, kSortTile);
+    for (int shift = 0; shift < 64; shift += 8) {
+        k_sort_hist<<<nb, kSortThreads, 0, st>>>(kin, n, shift, tb.sort_hist, nb);
+        L += 2 + scan_exclusive(tb.sort_hist, 256u * nb, tb.scan_tmp, nullptr, st);
+        k_sort_scatter<<<nb, kSortThreads, 0, st>>>(kin, iin, kout, iout, n, shift, tb.sort_hist, nb);
+        uint64_t *tk = kin; kin = kout; kout = tk;
+        uint32_t *ti = iin; iin = iout; iout = ti;
+    }
+    // 8 passes: the sorted data is back in key_a / idx_a
+    k_gather_bodies<<<blocks_for(n, 256), 256, 0, st>>>(tb.idx_a, tb.pos, tb.mass, tb.body, n);
+    L += 1;
+    *launches += L;
+    if (n < 2) return cudaGetLastError();
+    L = 0;
+    k_deep_groups<<<blocks_for(n, 256), 256, 0, st>>>(tb.key_a, tb.key2, tb.key3, tb.idx_a, tb.body, n,
+                                                       tb.sc);
+    KeyView kv{tb.key_a, tb.key2, tb.key3, (int)n};
+    const uint32_t m = n - 1;
+    k_radix_tree<<<blocks_for(m, 256), 256, 0, st>>>(kv, tb.bleft, tb.bright, tb.bparent, tb.leaf_bparent,
+                                                      tb.bdelta);
+    k_head_flags<<<blocks_for(m, 256), 256, 0, st>>>(tb.bparent, tb.bdelta, m, tb.head_flag);
+    cudaMemcpyAsync(tb.head_id, tb.head_flag, sizeof(uint32_t) * m, cudaMemcpyDeviceToDevice, st);
+    L += 3 + scan_exclusive(tb.head_id, m, tb.scan_tmp, &tb.sc->n_onodes, st);
+    // Parents default to "none" so a child the collapse could not attach
+    // (reported as an error) is never followed.
+    cudaMemsetAsync(tb.oparent, 0xff, sizeof(int32_t) * m, st);
+    cudaMemsetAsync(tb.leaf_oparent, 0xff, sizeof(int32_t) * n, st);
+    k_collapse<<<blocks_for(m, 256), 256, 0, st>>>(tb.bleft, tb.bright, tb.bdelta, tb.head_id, tb.head_flag,
+                                                    m, tb.ochild, tb.ometa, tb.oparent, tb.leaf_oparent,
+                                                    tb.sc);
+    L += 1;
+    *launches += L;
+    return cudaGetLastError();
+}
+
+cudaError_t compute_com(const TreeBuild &tb, cudaStream_t st, unsigned *launches) {
+    const uint32_t n = tb.n;
+    if (n < 2) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(tb.ocount, 0, sizeof(uint32_t) * (n - 1), st);
+    if (e != cudaSuccess) return e;
+    k_com<<<blocks_for(n, 256), 256, 0, st>>>(tb.body, tb.leaf_oparent, tb.oparent, tb.ochild, tb.ometa,
+                                              tb.onode, tb.ocount, n, tb.sc);
+    *launches += 1;
+    return cudaGetLastError();
+}
+
+}  // namespace nbody

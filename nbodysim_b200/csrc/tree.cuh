@@ -1,0 +1,35 @@
+// Octree construction: device buffers and the launch sequence (tree.cu).
+#pragma once
+
+#include "common.cuh"
+
+namespace nbody {
+
+struct TreeBuild {
+    uint32_t n;
+    const double *pos;          // user order, AoS
+    const double *mass;
+    const double *vel_for_max;  // non-null: also reduce max |v| (adaptive dt)
+    DevScalars *sc;
+    double *bbox_partial;       // 7 * bbox_blocks
+    unsigned bbox_blocks;
+    uint64_t *key_a, *key_b, *key2, *key3;
+    uint32_t *idx_a, *idx_b;
+    uint32_t *sort_hist;        // 256 * ceil(n / 4096)
+    uint32_t *scan_tmp;         // ceil(max_len / 4096) + 1
+    double4 *body;
+    int32_t *bleft, *bright, *bparent, *leaf_bparent, *bdelta;
+    uint32_t *head_flag, *head_id;
+    int32_t *ochild, *ometa, *oparent, *leaf_oparent;
+    uint32_t *ocount;
+    double4 *onode;
+};
+
+// Enqueues root cube -> keys -> sort -> bodies -> radix tree -> octree.
+cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launches);
+// Enqueues the bottom-up mass / centre-of-mass pass.
+cudaError_t compute_com(const TreeBuild &tb, cudaStream_t st, unsigned *launches);
+
+unsigned scan_exclusive(uint32_t *v, uint32_t len, uint32_t *tile_sums, uint32_t *total, cudaStream_t st);
+
+}  // namespace nbody

@@ -1,0 +1,77 @@
+"""Generates the golden fixtures in this folder from the reference's own code.
+
+Runs only where the reference tree is present and ``make -C oracle ref`` has
+built ``oracle/_ref/libnbref.so`` (fosted3/nbodysim's src/main.cpp, octree.cpp,
+particle.cpp, vector.cpp compiled unmodified, DOUBLE build). The outputs are
+small ``.npz`` files that pin the oracle (``oracle/bh_oracle.c``) where the
+reference is absent. Usage: ``python tests/golden/make_golden.py``.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+import oracle as O  # noqa: E402
+
+
+def lattice(k: int, step: float = 1.0):
+    """k^3 lattice centred on the origin; odd k puts particles on every split plane."""
+    r = (np.arange(k) - (k - 1) / 2.0) * step
+    g = np.stack(np.meshgrid(r, r, r, indexing="ij"), -1).reshape(-1, 3)
+    return np.ascontiguousarray(g), np.full(len(g), 1e10)
+
+
+def main() -> None:
+    R = O.Reference()
+    assert R.datatype_bytes == 8
+    out = {}
+    # seeded initial conditions: 64 particles per gen type x mass distribution
+    for gt in (O.CUBE, O.SPHERE, O.SHELL):
+        for md in (O.LINEAR, O.EXP, O.NORMAL):
+            g = O.GenParams(gen_type=gt, mass_dist=md, min_vel=1.0, max_vel=5.0)
+            p, v, m = R.generate(g, 64)
+            out[f"gen_{gt}_{md}_pos"] = p
+            out[f"gen_{gt}_{md}_vel"] = v
+            out[f"gen_{gt}_{md}_mass"] = m
+    np.savez_compressed(os.path.join(HERE, "generate.npz"), **out)
+
+    # forces on the default cube (config 1's generator), N = 512
+    pos, vel, mass = R.generate(O.GenParams(), 512)
+    out = dict(pos=pos, mass=mass)
+    for th in (0.3, 0.5, 0.7):
+        out[f"acc_{th}"] = R.forces(pos, mass, th)[0]
+    out["acc_damped_0.5"] = R.forces(pos, mass, 0.5, damping=True)[0]
+    np.savez_compressed(os.path.join(HERE, "forces_cube512.npz"), **out)
+
+    # sphere and shell, N = 512
+    for name, gt in (("sphere", O.SPHERE), ("shell", O.SHELL)):
+        pos, vel, mass = R.generate(O.GenParams(gen_type=gt, size=1024), 512)
+        np.savez_compressed(os.path.join(HERE, f"forces_{name}512.npz"), pos=pos, mass=mass,
+                            acc_0_5=R.forces(pos, mass, 0.5)[0])
+
+    # lattices: 3^3 (particles on the split planes: strict '>' decides), 4^3
+    for k in (3, 4):
+        pos, mass = lattice(k)
+        np.savez_compressed(os.path.join(HERE, f"forces_lattice{k}.npz"), pos=pos, mass=mass,
+                            acc_0_5=R.forces(pos, mass, 0.5)[0], acc_0_3=R.forces(pos, mass, 0.3)[0])
+
+    # five frames of the reference frame loop, cube N = 256
+    pos, vel, mass = R.generate(O.GenParams(), 256)
+    _, _, frames = R.run_frames(pos, vel, mass, 5, keep_frames=True)
+    np.savez_compressed(os.path.join(HERE, "frames_cube256.npz"), pos=pos, vel=vel, mass=mass, frames=frames)
+
+    # tree records (branching nodes), cube N = 512
+    pos, vel, mass = R.generate(O.GenParams(), 512)
+    t = R.tree_nodes(pos, mass)
+    np.savez_compressed(os.path.join(HERE, "tree_cube512.npz"), pos=pos, mass=mass,
+                        **{"node_" + k: np.asarray(v) for k, v in t.items()})
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,103 @@
+"""GPU: resident-state stepping, frame-loop parity, adaptive dt, diagnostics."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_frames_match_reference_fp64(nb, golden):
+    g = golden("frames_cube256.npz")
+    with nb.Engine(precision=nb.PRECISION_FP64) as e:
+        e.set_particles(g["pos"], g["vel"], g["mass"])
+        for f in range(5):
+            e.step(1)
+            p, v = e.get_particles()
+            err = np.abs(p - g["frames"][f]).max() / np.abs(g["frames"][f]).max()
+            assert err <= 1e-13, (f, err)
+
+
+def test_frames_match_oracle_mixed(nb, orc):
+    pos, vel, mass = nb.generate(2000)
+    _, _, frames = orc.run_frames(pos, vel, mass, 10, keep_frames=True)
+    with nb.Engine() as e:
+        e.set_particles(pos, vel, mass)
+        for f in range(10):
+            e.step(1)
+        p, v = e.get_particles()
+    err = np.linalg.norm(p - frames[-1], axis=1).max()
+    assert err <= 1e-6 * np.abs(frames[-1]).max(), err
+
+
+def test_step_host_equals_resident(nb):
+    pos, vel, mass = nb.generate(3000, gen_type=1)
+    with nb.Engine() as e:
+        e.set_particles(pos, vel, mass)
+        e.step(3)
+        p1, v1 = e.get_particles()
+        p2, v2 = pos.copy(), vel.copy()
+        e.step_host(p2, v2, mass, 3)
+    assert np.array_equal(p1, p2) and np.array_equal(v1, v2)
+
+
+def test_single_step_is_reference_update(nb, orc):
+    pos, vel, mass = nb.generate(4000, gen_type=1)
+    with nb.Engine(precision=nb.PRECISION_FP64) as e:
+        e.set_particles(pos, vel, mass)
+        e.step(1)
+        p, v = e.get_particles()
+    acc, _ = orc.forces(pos, mass, 0.5)
+    rp, rv = orc.update(pos, vel, acc, 0.0333)
+    assert np.abs(p - rp).max() <= 1e-12 * np.abs(rp).max()
+    assert np.abs(v - rv).max() <= 1e-10 * np.abs(rv).max()
+
+
+def test_adaptive_dt_rule(nb):
+    pos, vel, mass = nb.generate(5000, gen_type=2, size=1024)
+    with nb.Engine(adaptive=1, max_pos_change=0.05, max_vel_change=3.0, min_adaptive_dt=1e-4) as e:
+        acc = e.barnes_hut(pos, mass)
+        e.set_particles(pos, vel, mass)
+        e.step(1)
+        dt = e.stats()["last_dt"]
+    amax = np.linalg.norm(acc, axis=1).max()
+    vmax = np.linalg.norm(vel, axis=1).max()
+    expect = min(0.0333, 3.0 / amax, 0.05 / vmax)
+    expect = min(max(expect, 1e-4), 0.0333)
+    assert abs(dt - expect) <= 1e-6 * expect
+
+
+def test_diagnostics(nb, orc):
+    pos, vel, mass = nb.generate(3000, gen_type=1)
+    with nb.Engine() as e, nb.Engine(precision=nb.PRECISION_FP64) as e64:
+        e.set_particles(pos, vel, mass)
+        e64.set_particles(pos, vel, mass)
+        d = e.diagnostics()
+        d64 = e64.diagnostics()
+    ke = 0.5 * np.sum(mass * np.sum(vel * vel, 1))
+    assert abs(d["kinetic"] - ke) <= 1e-12 * ke
+    P = (mass[:, None] * vel).sum(0)
+    L = (mass[:, None] * np.cross(pos, vel)).sum(0)
+    assert np.allclose(d["momentum"], P, rtol=1e-10, atol=1e-10 * np.abs(mass[:, None] * vel).sum())
+    assert np.allclose(d["angular_momentum"], L, rtol=1e-10)
+    assert abs(d["mass"] - mass.sum()) <= 1e-12 * mass.sum()
+    # potential: mixed vs FP64 form, and vs direct-sum FP64 within the BH truncation
+    assert abs(d["potential"] - d64["potential"]) <= 1e-5 * abs(d64["potential"])
+    G = 6.67384e-11
+    r = np.linalg.norm(pos[:, None, :] - pos[None, :, :], axis=2)
+    np.fill_diagonal(r, np.inf)
+    pe = -0.5 * G * np.sum(mass[:, None] * mass[None, :] / r)
+    assert abs(d64["potential"] - pe) <= 1e-2 * abs(pe)
+
+
+def test_device_view(nb):
+    pos, vel, mass = nb.generate(100)
+    with nb.Engine() as e:
+        e.set_particles(pos, vel, mass)
+        v = e.device_view()
+        assert v.n == 100 and v.pos and v.vel and v.mass and v.acc and v.acc_is_double == 0
+
+
+def test_state_errors(nb):
+    with nb.Engine() as e:
+        with pytest.raises(nb.NBodyError) as ex:
+            e.step(1)
+        assert ex.value.status == nb.ERR_STATE

@@ -1,0 +1,93 @@
+"""The oracle (oracle/bh_oracle.c) pinned bit for bit to the reference's own code:
+against the committed golden fixtures (made by tests/golden/make_golden.py from
+the reference) and, where oracle/_ref was built, against the reference live."""
+import numpy as np
+import pytest
+
+
+def test_generator_matches_golden(orc, oracle_mod, golden):
+    g = golden("generate.npz")
+    for gt in (0, 1, 2):
+        for md in (0, 1, 2):
+            p, v, m = orc.generate(oracle_mod.GenParams(gen_type=gt, mass_dist=md, min_vel=1.0, max_vel=5.0), 64)
+            assert np.array_equal(p, g[f"gen_{gt}_{md}_pos"])
+            assert np.array_equal(v, g[f"gen_{gt}_{md}_vel"])
+            assert np.array_equal(m, g[f"gen_{gt}_{md}_mass"])
+
+
+@pytest.mark.parametrize("theta", [0.3, 0.5, 0.7])
+def test_forces_cube_golden(orc, golden, theta):
+    g = golden("forces_cube512.npz")
+    acc, _ = orc.forces(g["pos"], g["mass"], theta)
+    assert np.array_equal(acc, g[f"acc_{theta}"])
+
+
+def test_forces_damped_golden(orc, golden):
+    g = golden("forces_cube512.npz")
+    acc, _ = orc.forces(g["pos"], g["mass"], 0.5, damping=True)
+    assert np.array_equal(acc, g["acc_damped_0.5"])
+
+
+@pytest.mark.parametrize("name", ["sphere512", "shell512"])
+def test_forces_sphere_shell_golden(orc, golden, name):
+    g = golden(f"forces_{name}.npz")
+    acc, _ = orc.forces(g["pos"], g["mass"], 0.5)
+    assert np.array_equal(acc, g["acc_0_5"])
+
+
+@pytest.mark.parametrize("k", [3, 4])
+def test_forces_lattice_golden(orc, golden, k):
+    """Lattice with particles exactly on split planes: the strict '>' octant rule."""
+    g = golden(f"forces_lattice{k}.npz")
+    for th, key in ((0.5, "acc_0_5"), (0.3, "acc_0_3")):
+        acc, _ = orc.forces(g["pos"], g["mass"], th)
+        assert np.array_equal(acc, g[key])
+
+
+def test_frames_golden(orc, golden):
+    g = golden("frames_cube256.npz")
+    _, _, frames = orc.run_frames(g["pos"], g["vel"], g["mass"], 5, keep_frames=True)
+    assert np.array_equal(frames, g["frames"])
+
+
+def test_tree_records_golden(orc, golden):
+    g = golden("tree_cube512.npz")
+    t = orc.tree_nodes(g["pos"], g["mass"])
+    for k in ("level", "count", "min_index", "mass", "com", "side"):
+        assert np.array_equal(t[k], g["node_" + k]), k
+    assert t["depth"] == int(g["node_depth"])
+
+
+def test_root_cube_tie_rule(orc):
+    # equal x and y extents larger than z: the reference falls through to z (src/main.cpp:909-920)
+    pos = np.array([[0, 0, 0], [4, 4, 1]], float)
+    c, s = orc.root_cube(pos)
+    assert np.allclose(c, [2, 2, 0.5]) and s == 3.0
+
+
+def test_direct_sum_two_body(orc):
+    pos = np.array([[0.0, 0, 0], [2.0, 0, 0]])
+    mass = np.array([1e10, 3e10])
+    a = orc.direct(pos, mass)
+    G = 6.67384e-11
+    assert np.allclose(a[0], [G * 3e10 / 4, 0, 0], rtol=1e-15)
+    assert np.allclose(a[1], [-G * 1e10 / 4, 0, 0], rtol=1e-15)
+
+
+@pytest.mark.parametrize("gt,n,theta,damp", [(0, 3000, 0.5, False), (1, 3000, 0.3, False),
+                                             (2, 3000, 0.7, True), (0, 2000, 0.5, True)])
+def test_oracle_equals_reference_live(orc, ref, oracle_mod, gt, n, theta, damp):
+    g = oracle_mod.GenParams(gen_type=gt, size=1024 if gt else 512)
+    p, v, m = ref.generate(g, n)
+    q = orc.generate(g, n)
+    assert all(np.array_equal(a, b) for a, b in zip((p, v, m), q))
+    a_ref, _ = ref.forces(p, m, theta, damping=damp)
+    a_or, _ = orc.forces(p, m, theta, damping=damp)
+    assert np.array_equal(a_ref, a_or)
+
+
+def test_oracle_frames_equal_reference_live(orc, ref, oracle_mod):
+    p, v, m = ref.generate(oracle_mod.GenParams(gen_type=1), 800)
+    _, _, f1 = ref.run_frames(p, v, m, 4, keep_frames=True)
+    _, _, f2 = orc.run_frames(p, v, m, 4, keep_frames=True)
+    assert np.array_equal(f1, f2)
