@@ -121,6 +121,10 @@ typedef struct nbody_stats {
     uint64_t interactions;   /* accepted (particle, node) pairs in the last force pass */
     uint64_t interactions_total; /* summed over every pass of the last API call */
     uint64_t kernel_launches;    /* kernels this context has enqueued since creation */
+    uint64_t walk_entries;       /* node entries tested by the walk's warps in the last pass */
+    uint64_t walk_tiles;         /* stack tiles (<= 32 entries) the walk's warps staged */
+    uint64_t walk_decisions;     /* internal nodes the warps decided (open / accept) */
+    uint64_t walk_list;          /* bodies the warps put in their interaction lists */
     uint32_t tree_nodes;     /* internal nodes of the (chain-free) octree */
     uint32_t tree_depth;     /* deepest internal-node level */
     uint32_t max_stack;      /* deepest walk stack seen (entries) */

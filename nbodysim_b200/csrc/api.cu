@@ -155,6 +155,10 @@ int check_status(nbody_ctx *c) {
     nbody_stats &s = c->stats;
     s.interactions = h.interactions;
     s.interactions_total = h.interactions_total;
+    s.walk_entries = h.walk_entries;
+    s.walk_tiles = h.walk_tiles;
+    s.walk_decisions = h.walk_decisions;
+    s.walk_list = h.walk_list;
     s.kernel_launches = c->launches;
     s.tree_nodes = h.n_onodes;
     s.tree_depth = h.depth;

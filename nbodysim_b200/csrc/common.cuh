@@ -39,6 +39,10 @@ struct DevScalars {
     double bbox_max[3];
     unsigned long long interactions;
     unsigned long long interactions_total;  // summed over the steps of one API call
+    unsigned long long walk_entries;        // node entries the walk warps tested (union lists)
+    unsigned long long walk_tiles;          // stack tiles the walk warps staged
+    unsigned long long walk_decisions;      // internal nodes decided by a warp
+    unsigned long long walk_list;           // bodies entered in the warps' interaction lists
     uint32_t status;
     uint32_t n_onodes;
     uint32_t depth;
@@ -77,6 +81,14 @@ __device__ inline double warp_min(double v) {
 }
 __device__ inline double warp_max(double v) {
     for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ inline float warp_minf(float v) {
+    for (int o = 16; o; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ inline float warp_maxf(float v) {
+    for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
 }
 __device__ inline double warp_sum(double v) {

@@ -91,6 +91,10 @@ __global__ void k_diag(const double *__restrict__ pos, const double *__restrict_
 
 __global__ void k_reset_pass(DevScalars *sc) {
     sc->interactions = 0;
+    sc->walk_entries = 0;
+    sc->walk_tiles = 0;
+    sc->walk_decisions = 0;
+    sc->walk_list = 0;
     sc->n_onodes = 0;
     sc->depth = 0;
     sc->max_stack = 0;

@@ -40,27 +40,31 @@ __device__ inline double exp2_neg(int L) {  // exactly 2^-L for 0 <= L <= 1022
     return __longlong_as_double((long long)(1023 - L) << 52);
 }
 
+// Per-warp shared memory. The stack holds nodes still to be examined with
+// the mask of lanes that reached them; the tile holds the up-to-32 internal
+// nodes being decided; the list holds accepted bodies (internal nodes a lane
+// did not open, and leaves) with the mask of lanes that take them.
 template <bool kFp64>
-struct WarpTiles;
+struct WarpSmem;
 
 template <>
-struct WarpTiles<false> {
+struct WarpSmem<false> {
     int2 stack[kStackCap];
-    float4 c[32];      // (com - ref).xyz, G m
-    float4 q[32];      // q = (side/theta)^2, sqrt(q), 32u q, -
-    int2 r[32];        // node ref, reach mask
-    int child[32][8];  // children of internal entries
-    int nch[32];
+    float4 tc[32];            // (com - ref).xyz, -
+    float4 tq[32];            // q = (side/theta)^2, band half-width, reach mask bits, node ref bits
+    int child[32][8];
+    float4 lc[kListCap];      // (com - ref).xyz, G m
+    uint32_t lm[kListCap];
 };
 
 template <>
-struct WarpTiles<true> {
+struct WarpSmem<true> {
     int2 stack[kStackCap];
-    double4 c[32];     // com.xyz (absolute), G m
-    double side[32];   // node side (internal), -1 for leaves
-    int2 r[32];
+    double4 tc[32];           // com.xyz (absolute), side
+    int2 tr[32];              // reach mask, node ref
     int child[32][8];
-    int nch[32];
+    double4 lc[kListCap];     // com.xyz (absolute), G m
+    uint32_t lm[kListCap];
 };
 
 // The reference's FP64 opening test on the original doubles
@@ -73,9 +77,9 @@ __device__ inline bool exact_open(double cx, double cy, double cz, double px, do
 }
 
 // Moves the oldest half of a full stack to this warp's global spill region.
-template <class Tiles>
-__device__ inline bool spill_out(Tiles &s, int &top, uint32_t &spill_top, int2 *gspill,
-                                 uint32_t spill_cap, int lane) {
+template <class Sm>
+__device__ inline bool spill_out(Sm &s, int &top, uint32_t &spill_top, int2 *gspill, uint32_t spill_cap,
+                                 int lane) {
     if (spill_top + kSpillChunk > spill_cap) return false;
     for (int e = lane; e < kSpillChunk; e += 32) gspill[spill_top + e] = s.stack[e];
     __syncwarp();
@@ -86,8 +90,8 @@ __device__ inline bool spill_out(Tiles &s, int &top, uint32_t &spill_top, int2 *
     return true;
 }
 
-template <class Tiles>
-__device__ inline void spill_in(Tiles &s, int &top, uint32_t &spill_top, const int2 *gspill, int lane) {
+template <class Sm>
+__device__ inline void spill_in(Sm &s, int &top, uint32_t &spill_top, const int2 *gspill, int lane) {
     int take = min((int)spill_top, kSpillChunk);
     for (int e = lane; e < take; e += 32) s.stack[e] = gspill[spill_top - take + e];
     __syncwarp();
@@ -95,12 +99,62 @@ __device__ inline void spill_in(Tiles &s, int &top, uint32_t &spill_top, const i
     top = take;
 }
 
+// Gravity of the listed bodies on each lane's particle: a lane takes an entry
+// iff its bit is set in the entry's mask.
+template <bool kDamp, bool kPot>
+__device__ inline void force_list_f32(const float4 *lc, const uint32_t *lm, int count, int lane, float px,
+                                      float py, float pz, float &ax, float &ay, float &az, float &pot,
+                                      uint32_t &cnt) {
+#pragma unroll 4
+    for (int k = 0; k < count; k++) {
+        const float4 c = lc[k];
+        const bool take = (lm[k] >> lane) & 1u;
+        const float dx = c.x - px, dy = c.y - py, dz = c.z - pz;
+        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+        const float inv = rsqrtf(r2);
+        float f;
+        if constexpr (kDamp) {
+            const float r = r2 * inv;
+            f = c.w * inv / (r2 + expf(-r));
+        } else {
+            f = c.w * inv * (inv * inv);
+        }
+        if (take) {
+            ax = fmaf(f, dx, ax); ay = fmaf(f, dy, ay); az = fmaf(f, dz, az);
+            if constexpr (kPot) pot = fmaf(c.w, inv, pot);
+            cnt++;
+        }
+    }
+}
+
+template <bool kDamp, bool kPot>
+__device__ inline void force_list_f64(const double4 *lc, const uint32_t *lm, int count, int lane, double bx,
+                                      double by, double bz, double &ax, double &ay, double &az, double &pot,
+                                      uint32_t &cnt) {
+#pragma unroll 2
+    for (int k = 0; k < count; k++) {
+        const uint32_t m = lm[k];
+        if (!((m >> lane) & 1u)) continue;
+        const double4 c = lc[k];
+        const double dx = c.x - bx, dy = c.y - by, dz = c.z - bz;
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        const double d = sqrt(r2);
+        const double inv = 1.0 / d;
+        double f;
+        if constexpr (kDamp) f = c.w * inv / (r2 + exp(-d));
+        else f = c.w * inv * inv * inv;
+        ax = fma(f, dx, ax); ay = fma(f, dy, ay); az = fma(f, dz, az);
+        if constexpr (kPot) pot += c.w * inv;
+        cnt++;
+    }
+}
+
 template <bool kFp64, bool kDamp, bool kPot>
 __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    using Tiles = WarpTiles<kFp64>;
+    using Sm = WarpSmem<kFp64>;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    Tiles &s = reinterpret_cast<Tiles *>(smem_raw)[wid];
+    Sm &s = reinterpret_cast<Sm *>(smem_raw)[wid];
     const Tree &t = a.t;
     const uint32_t n = t.n;
     const double S = t.sc->root_side;
@@ -108,6 +162,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
     const double s_theta = S / theta;
     int2 *gspill = a.spill + (size_t)(blockIdx.x * kWalkWarps + wid) * a.spill_cap;
     const unsigned FULL = 0xffffffffu;
+    const uint32_t lt = (1u << lane) - 1u;
 
     for (;;) {
         uint32_t g = 0;
@@ -115,9 +170,10 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
         g = __shfl_sync(FULL, g, 0);
         if (g >= a.n_groups) break;
 
-        const uint32_t j = g * 32 + lane;
+        const uint32_t g0 = g * 32;
+        const uint32_t j = g0 + lane;
         const bool valid = j < n;
-        const double4 b = t.body[valid ? j : g * 32];
+        const double4 b = t.body[valid ? j : g0];
         const uint32_t vmask = __ballot_sync(FULL, valid);
 
         // Reference point: centre of the group's bounding box.
@@ -125,20 +181,34 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
         const double ry = 0.5 * (warp_min(b.y) + warp_max(b.y));
         const double rz = 0.5 * (warp_min(b.z) + warp_max(b.z));
         const float px = (float)(b.x - rx), py = (float)(b.y - ry), pz = (float)(b.z - rz);
-        // Error band of the FP32 test (walk_band): with u = 2^-24 and Pm the
-        // largest |offset| of this particle, |r2_f32 - r2| <= 7.1u r2 + 7u Pm sqrt(r2)
-        // and |q_f32 - q| <= 1.01u q, so outside |r2 - q| <= 32u q + 20u Pm sqrt(q)
-        // and r2 > (64u Pm)^2 the FP32 decision equals the exact one.
-        const float pm = fmaxf(fabsf(px), fmaxf(fabsf(py), fabsf(pz)));
-        const float pm_tol = kTolPm * pm;
-        const float tiny = (kTiny * pm) * (kTiny * pm);
+        // Error band of the FP32 opening test. With u = 2^-24 and Pm the largest
+        // |offset| from the reference point in the group, every lane has
+        // |r2_f32 - r2| <= 7.1u r2 + 7u Pm sqrt(r2) and |q_f32 - q| <= 1.01u q;
+        // outside |r2 - q| <= 32u q + 20u Pm sqrt(q), and for r2 > (64u Pm)^2,
+        // the FP32 decision equals the exact one. Inside, the lane re-tests in FP64.
+        const float pm_g = warp_maxf(fmaxf(fabsf(px), fmaxf(fabsf(py), fabsf(pz))));
+        const float pm_tol = kTolPm * pm_g;
+        const float tiny = (kTiny * pm_g) * (kTiny * pm_g);
+        // Group bounding box of the offsets (lanes past n repeat lane 0): FP32
+        // for the MIXED form, FP64 for the FP64 form (group-level test only).
+        float lox = 0.f, hix = 0.f, loy = 0.f, hiy = 0.f, loz = 0.f, hiz = 0.f;
+        double dlox = 0.0, dhix = 0.0, dloy = 0.0, dhiy = 0.0, dloz = 0.0, dhiz = 0.0, dpm = 0.0;
+        if constexpr (kFp64) {
+            dlox = warp_min(b.x) - rx; dhix = warp_max(b.x) - rx;
+            dloy = warp_min(b.y) - ry; dhiy = warp_max(b.y) - ry;
+            dloz = warp_min(b.z) - rz; dhiz = warp_max(b.z) - rz;
+            dpm = fmax(fmax(fmax(-dlox, dhix), fmax(-dloy, dhiy)), fmax(-dloz, dhiz));
+        } else {
+            lox = warp_minf(px); hix = warp_maxf(px);
+            loy = warp_minf(py); hiy = warp_maxf(py);
+            loz = warp_minf(pz); hiz = warp_maxf(pz);
+        }
 
         float fax = 0.f, fay = 0.f, faz = 0.f, fpot = 0.f;
         double dax = 0.0, day = 0.0, daz = 0.0, dpot = 0.0;
-        uint32_t cnt = 0, nfallback = 0;
-        int top = 0;
+        uint32_t cnt = 0, nfallback = 0, nentries = 0, ntiles = 0, ndecide = 0, nlist = 0;
+        int top = 0, list_top = 0, max_top = 0;
         uint32_t spill_top = 0;
-        int max_top = 0;
         bool failed = false;
         if (n >= 2) {
             if (lane == 0) s.stack[0] = make_int2(0, (int)vmask);
@@ -151,124 +221,183 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
             const int cntt = min(top, 32);
             const int base = top - cntt;
             top = base;
-            // ---- stage a tile of up to 32 stacked nodes in shared memory
+            nentries += cntt;
+            ntiles++;
+
+            // ---- stage: lane k takes stack entry k
+            bool is_int = false;
+            uint32_t reach = 0;
+            int nch = 0, ref = 0;
+            double cx = 0, cy = 0, cz = 0, m = 0, so = 0;
             if (lane < cntt) {
                 const int2 e = s.stack[base + lane];
-                double cx, cy, cz, m;
-                int nch = 0;
-                double so = -1.0;
-                if (e.x >= 0) {
-                    const double4 nd = t.onode[e.x];
-                    const int meta = t.ometa[e.x];
+                ref = e.x;
+                reach = (uint32_t)e.y;
+                if (ref >= 0) {
+                    const double4 nd = t.onode[ref];
+                    const int meta = t.ometa[ref];
                     cx = nd.x; cy = nd.y; cz = nd.z; m = nd.w;
                     nch = meta_nchild(meta);
-                    const double sc2 = exp2_neg(meta_level(meta));
-                    so = kFp64 ? S * sc2 : s_theta * sc2;
-                    const int4 *cp = reinterpret_cast<const int4 *>(t.ochild + 8 * (size_t)e.x);
+                    so = exp2_neg(meta_level(meta));  // 2^-level
+                    const int4 *cp = reinterpret_cast<const int4 *>(t.ochild + 8 * (size_t)ref);
                     const int4 c0 = cp[0], c1 = cp[1];
                     s.child[lane][0] = c0.x; s.child[lane][1] = c0.y;
                     s.child[lane][2] = c0.z; s.child[lane][3] = c0.w;
                     s.child[lane][4] = c1.x; s.child[lane][5] = c1.y;
                     s.child[lane][6] = c1.z; s.child[lane][7] = c1.w;
+                    is_int = true;
                 } else {
-                    const double4 bd = t.body[~e.x];
+                    const double4 bd = t.body[~ref];
                     cx = bd.x; cy = bd.y; cz = bd.z; m = bd.w;
+                    const uint32_t own = (uint32_t)(~ref) - g0;  // a leaf of this group: not its own lane
+                    if (own < 32u) reach &= ~(1u << own);
                 }
+            }
+            float fcx = 0.f, fcy = 0.f, fcz = 0.f;
+            if constexpr (!kFp64) {
+                fcx = (float)(cx - rx); fcy = (float)(cy - ry); fcz = (float)(cz - rz);
+            }
+
+            // ---- group-level test, one node per lane: when every point of the
+            // group's box (widened by twice the FP32 error band) lies beyond the
+            // opening radius side/theta, no lane opens the node; when every point
+            // lies within it, every lane that reached it opens it. Only the
+            // remaining nodes are decided lane by lane below.
+            uint32_t my_open = 0;
+            bool mixed = false;
+            if (is_int) {
                 if constexpr (kFp64) {
-                    s.c[lane] = make_double4(cx, cy, cz, kG * m);
-                    s.side[lane] = so;  // node side, or -1 for a leaf
+                    const double sq = S * so / theta;
+                    const double qd = sq * sq;
+                    const double ox = cx - rx, oy = cy - ry, oz = cz - rz;
+                    const double ax_ = fmax(fmax(dlox - ox, ox - dhix), 0.0), ay_ = fmax(fmax(dloy - oy, oy - dhiy), 0.0),
+                                 az_ = fmax(fmax(dloz - oz, oz - dhiz), 0.0);
+                    const double bx_ = fmax(fabs(ox - dlox), fabs(ox - dhix)), by_ = fmax(fabs(oy - dloy), fabs(oy - dhiy)),
+                                 bz_ = fmax(fabs(oz - dloz), fabs(oz - dhiz));
+                    const double r2min = ax_ * ax_ + ay_ * ay_ + az_ * az_;
+                    const double r2max = bx_ * bx_ + by_ * by_ + bz_ * bz_;
+                    const double tol = 1e-12 * (qd + dpm * sq) + 1e-300;
+                    if (r2min - qd > tol) my_open = 0;
+                    else if (qd - r2max > tol) my_open = reach;
+                    else mixed = true;
                 } else {
-                    s.c[lane] = make_float4((float)(cx - rx), (float)(cy - ry), (float)(cz - rz),
-                                            (float)(kG * m));
-                    if (so > 0.0) {
-                        const float qf = (float)(so * so);
-                        s.q[lane] = make_float4(qf, (float)so, kTolRel * qf, 0.f);
+                    const double sqd = s_theta * so;
+                    const float qf = (float)(sqd * sqd), sqf = (float)sqd;
+                    const float tol = 2.f * fmaf(pm_tol, sqf, kTolRel * qf);
+                    const float ax_ = fmaxf(fmaxf(lox - fcx, fcx - hix), 0.f), ay_ = fmaxf(fmaxf(loy - fcy, fcy - hiy), 0.f),
+                                az_ = fmaxf(fmaxf(loz - fcz, fcz - hiz), 0.f);
+                    const float bx_ = fmaxf(fabsf(fcx - lox), fabsf(fcx - hix)), by_ = fmaxf(fabsf(fcy - loy), fabsf(fcy - hiy)),
+                                bz_ = fmaxf(fabsf(fcz - loz), fabsf(fcz - hiz));
+                    const float r2min = fmaf(az_, az_, fmaf(ay_, ay_, ax_ * ax_));
+                    const float r2max = fmaf(bz_, bz_, fmaf(by_, by_, bx_ * bx_));
+                    if (r2min <= 4.f * tiny) mixed = true;
+                    else if (r2min - qf > tol) my_open = 0;
+                    else if (qf - r2max > tol) my_open = reach;
+                    else mixed = true;
+                }
+            }
+
+            // ---- decide the mixed nodes of the tile, lane by lane
+            const uint32_t intm = __ballot_sync(FULL, mixed);
+            ndecide += __popc(intm);
+            if (intm) {
+                if constexpr (kFp64) {
+                    s.tc[lane] = make_double4(cx, cy, cz, S * so);
+                    s.tr[lane] = make_int2((int)reach, ref);
+                } else {
+                    const double sq = s_theta * so;
+                    const float qf = (float)(sq * sq);
+                    s.tc[lane] = make_float4(fcx, fcy, fcz, 0.f);
+                    s.tq[lane] = make_float4(qf, fmaf(pm_tol, (float)sq, kTolRel * qf), __uint_as_float(reach),
+                                             __int_as_float(ref));
+                }
+                __syncwarp();
+                uint32_t mm = intm;
+                while (mm) {
+                    const int k = __ffs(mm) - 1;
+                    mm &= mm - 1;
+                    bool open;
+                    uint32_t rk;
+                    if constexpr (kFp64) {
+                        const double4 c = s.tc[k];
+                        const int2 tr = s.tr[k];
+                        rk = (uint32_t)tr.x;
+                        const double dx = __dsub_rn(c.x, b.x), dy = __dsub_rn(c.y, b.y), dz = __dsub_rn(c.z, b.z);
+                        const double d = __dsqrt_rn(
+                            __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+                        open = __ddiv_rn(c.w, d) > theta;
                     } else {
-                        s.q[lane] = make_float4(-1.f, 0.f, 0.f, 0.f);
-                    }
-                }
-                s.r[lane] = e;
-                s.nch[lane] = nch;
-            }
-            __syncwarp();
-            // ---- every lane tests every node of the tile against its particle
-            for (int k = 0; k < cntt; k++) {
-                const int2 rm = s.r[k];
-                const bool reached = (rm.y >> lane) & 1;
-                bool open = false;
-                bool take;
-                if constexpr (kFp64) {
-                    const double4 c = s.c[k];
-                    const double dx = __dsub_rn(c.x, b.x), dy = __dsub_rn(c.y, b.y),
-                                 dz = __dsub_rn(c.z, b.z);
-                    const double r2 =
-                        __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-                    double d = -1.0;
-                    if (rm.x >= 0) {
-                        d = __dsqrt_rn(r2);
-                        open = __ddiv_rn(s.side[k], d) > theta;
-                    }
-                    take = reached && !open && rm.x != (int)~j;
-                    if (__any_sync(FULL, take) && take) {
-                        if (d < 0.0) d = sqrt(r2);
-                        const double inv = 1.0 / d;
-                        double f;
-                        if constexpr (kDamp) f = c.w * inv / (r2 + exp(-d));
-                        else f = c.w * inv * inv * inv;
-                        dax = fma(f, dx, dax); day = fma(f, dy, day); daz = fma(f, dz, daz);
-                        if constexpr (kPot) dpot += c.w * inv;
-                        cnt++;
-                    }
-                } else {
-                    const float4 c = s.c[k];
-                    const float dx = c.x - px, dy = c.y - py, dz = c.z - pz;
-                    const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                    if (rm.x >= 0) {
-                        const float4 q = s.q[k];
-                        const float dq = r2 - q.x;
-                        open = dq < 0.f;
-                        const bool amb = reached && (fabsf(dq) <= fmaf(pm_tol, q.y, q.z) || r2 <= tiny);
-                        if (__any_sync(FULL, amb) && amb) {
-                            const double4 nd = t.onode[rm.x];
-                            const double side = S * exp2_neg(meta_level(t.ometa[rm.x]));
-                            open = exact_open(nd.x, nd.y, nd.z, b.x, b.y, b.z, side, theta);
-                            nfallback++;
+                        const float4 c = s.tc[k];
+                        const float4 q = s.tq[k];
+                        rk = __float_as_uint(q.z);
+                        const float dx = c.x - px, dy = c.y - py, dz = c.z - pz;
+                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                        const float d = r2 - q.x;
+                        open = d < 0.f;
+                        const bool amb = ((rk >> lane) & 1u) && (fabsf(d) <= q.y || r2 <= tiny);
+                        if (__any_sync(FULL, amb)) {
+                            if (amb) {
+                                const int node = __float_as_int(q.w);
+                                const double4 nd = t.onode[node];
+                                const double side = S * exp2_neg(meta_level(t.ometa[node]));
+                                open = exact_open(nd.x, nd.y, nd.z, b.x, b.y, b.z, side, theta);
+                                nfallback++;
+                            }
                         }
                     }
-                    take = reached && !open && rm.x != (int)~j;
-                    if (__any_sync(FULL, take) && take) {
-                        const float inv = rsqrtf(r2);
-                        float f;
-                        if constexpr (kDamp) {
-                            const float r = r2 * inv;
-                            f = c.w * inv / (r2 + expf(-r));
-                        } else {
-                            f = c.w * inv * inv * inv;
-                        }
-                        fax = fmaf(f, dx, fax); fay = fmaf(f, dy, fay); faz = fmaf(f, dz, faz);
-                        if constexpr (kPot) fpot = fmaf(c.w, inv, fpot);
-                        cnt++;
-                    }
-                }
-                const uint32_t openm = __ballot_sync(FULL, reached && open);
-                if (openm) {
-                    const int nch = s.nch[k];
-                    if (top + nch > kStackCap) {
-                        if (!spill_out(s, top, spill_top, gspill, a.spill_cap, lane)) {
-                            failed = true;
-                            break;
-                        }
-                    }
-                    if (lane < nch) s.stack[top + lane] = make_int2(s.child[k][lane], (int)openm);
-                    top += nch;
-                    max_top = max(max_top, top + (int)spill_top);
-                    __syncwarp();
+                    const uint32_t om = __ballot_sync(FULL, open) & rk;
+                    if (lane == k) my_open = om;
                 }
             }
+
+            // ---- accepted bodies -> interaction list (compacted across lanes)
+            const uint32_t accm = reach & ~my_open;
+            const uint32_t am = __ballot_sync(FULL, accm != 0);
+            if (accm) {
+                const int pos = list_top + __popc(am & lt);
+                if constexpr (kFp64) s.lc[pos] = make_double4(cx, cy, cz, kG * m);
+                else s.lc[pos] = make_float4(fcx, fcy, fcz, (float)(kG * m));
+                s.lm[pos] = accm;
+            }
+            list_top += __popc(am);
+            nlist += __popc(am);
+
+            // ---- children of opened nodes -> stack
+            const int myn = my_open ? nch : 0;
+            int pre = myn;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(FULL, pre, o);
+                if (lane >= o) pre += y;
+            }
+            const int total = __shfl_sync(FULL, pre, 31);
+            pre -= myn;
+            if (total > 0) {
+                if (top + total > kStackCap) {
+                    if (!spill_out(s, top, spill_top, gspill, a.spill_cap, lane)) {
+                        failed = true;
+                        break;
+                    }
+                }
+                for (int i = 0; i < myn; i++) s.stack[top + pre + i] = make_int2(s.child[lane][i], (int)my_open);
+                top += total;
+                max_top = max(max_top, top + (int)spill_top);
+            }
             __syncwarp();
-            if (failed) break;
+
+            // ---- forces once the list is long enough
+            if (list_top >= kListFlush) {
+                if constexpr (kFp64) force_list_f64<kDamp, kPot>(s.lc, s.lm, list_top, lane, b.x, b.y, b.z, dax, day, daz, dpot, cnt);
+                else force_list_f32<kDamp, kPot>(s.lc, s.lm, list_top, lane, px, py, pz, fax, fay, faz, fpot, cnt);
+                list_top = 0;
+                __syncwarp();
+            }
         }
         if (failed && lane == 0) atomicOr(&t.sc->status, kStatusCapacity);
+        if (list_top > 0) {
+            if constexpr (kFp64) force_list_f64<kDamp, kPot>(s.lc, s.lm, list_top, lane, b.x, b.y, b.z, dax, day, daz, dpot, cnt);
+            else force_list_f32<kDamp, kPot>(s.lc, s.lm, list_top, lane, px, py, pz, fax, fay, faz, fpot, cnt);
+        }
+        __syncwarp();
 
         // ---- epilogue: results in the caller's particle order
         double ax, ay, az;
@@ -286,7 +415,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
                 if (a.pot) a.pot[ui] = kFp64 ? -dpot : -(double)fpot;
             }
         }
-        unsigned long long wc = cnt;
+        unsigned long long wc = valid ? cnt : 0u;
         for (int o = 16; o; o >>= 1) wc += __shfl_xor_sync(FULL, wc, o);
         uint32_t wf = nfallback;
         for (int o = 16; o; o >>= 1) wf += __shfl_xor_sync(FULL, wf, o);
@@ -296,10 +425,13 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
             atomicAdd(&t.sc->interactions, wc);
             atomicAdd(&t.sc->interactions_total, wc);
             if (wf) atomicAdd(&t.sc->fallback_tests, wf);
+            atomicAdd(&t.sc->walk_entries, (unsigned long long)nentries);
+            atomicAdd(&t.sc->walk_tiles, (unsigned long long)ntiles);
+            atomicAdd(&t.sc->walk_decisions, (unsigned long long)ndecide);
+            atomicAdd(&t.sc->walk_list, (unsigned long long)nlist);
             atomicMax(&t.sc->max_stack, (uint32_t)max_top);
             if (a.track_max_acc) atomic_max_nonneg(&t.sc->max_acc_bits, amag);
         }
-        (void)vmask;
     }
 }
 
@@ -312,7 +444,7 @@ const void *walk_kernel(int damping, bool pot) {
 }  // namespace
 
 cudaError_t walk_launch_shape(bool fp64, int device, WalkLaunch *out) {
-    const size_t smem = (fp64 ? sizeof(WarpTiles<true>) : sizeof(WarpTiles<false>)) * kWalkWarps;
+    const size_t smem = (fp64 ? sizeof(WarpSmem<true>) : sizeof(WarpSmem<false>)) * kWalkWarps;
     const void *kernels[8] = {
         (const void *)k_walk<false, false, false>, (const void *)k_walk<false, false, true>,
         (const void *)k_walk<false, true, false>, (const void *)k_walk<false, true, true>,

@@ -6,8 +6,10 @@
 namespace nbody {
 
 constexpr int kWalkWarps = 4;       // warps per block
-constexpr int kStackCap = 1024;     // shared-memory stack entries per warp
+constexpr int kStackCap = 768;      // shared-memory stack entries per warp
 constexpr int kSpillChunk = kStackCap / 2;
+constexpr int kListFlush = 32;      // force pass once the interaction list holds this many
+constexpr int kListCap = kListFlush + 32;
 
 struct WalkArgs {
     Tree t;
