@@ -118,6 +118,8 @@ _SIGS = {
     "nbody_status_string": (C.c_char_p, [C.c_int]),
     "nbody_last_error_message": (C.c_char_p, []),
     "nbody_probe_fp32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "nbody_root_cube_noalloc_max_n": (C.c_uint32, []),
+    "nbody_root_cube_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None
