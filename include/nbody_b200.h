@@ -125,6 +125,7 @@ typedef struct nbody_stats {
     uint64_t walk_tiles;         /* stack tiles (<= 32 entries) the walk's warps staged */
     uint64_t walk_decisions;     /* internal nodes the warps decided (open / accept) */
     uint64_t walk_list;          /* bodies the warps put in their interaction lists */
+    uint64_t walk_near;          /* bodies taken with FP64 offsets (too close for FP32 offsets) */
     uint32_t tree_nodes;     /* internal nodes of the (chain-free) octree */
     uint32_t tree_depth;     /* deepest internal-node level */
     uint32_t max_stack;      /* deepest walk stack seen (entries) */

@@ -65,7 +65,7 @@ class Stats(C.Structure):
     _fields_ = [
         ("interactions", C.c_uint64), ("interactions_total", C.c_uint64), ("kernel_launches", C.c_uint64),
         ("walk_entries", C.c_uint64), ("walk_tiles", C.c_uint64), ("walk_decisions", C.c_uint64),
-        ("walk_list", C.c_uint64),
+        ("walk_list", C.c_uint64), ("walk_near", C.c_uint64),
         ("tree_nodes", C.c_uint32), ("tree_depth", C.c_uint32),
         ("max_stack", C.c_uint32), ("fallback_tests", C.c_uint32), ("last_dt", C.c_double),
         ("root_center", C.c_double * 3), ("root_side", C.c_double),

@@ -159,6 +159,7 @@ int check_status(nbody_ctx *c) {
     s.walk_tiles = h.walk_tiles;
     s.walk_decisions = h.walk_decisions;
     s.walk_list = h.walk_list;
+    s.walk_near = h.walk_near;
     s.kernel_launches = c->launches;
     s.tree_nodes = h.n_onodes;
     s.tree_depth = h.depth;

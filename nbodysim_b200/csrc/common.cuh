@@ -43,6 +43,7 @@ struct DevScalars {
     unsigned long long walk_tiles;          // stack tiles the walk warps staged
     unsigned long long walk_decisions;      // internal nodes decided by a warp
     unsigned long long walk_list;           // bodies entered in the warps' interaction lists
+    unsigned long long walk_near;           // bodies taken with FP64 offsets (near the group box)
     uint32_t status;
     uint32_t n_onodes;
     uint32_t depth;

@@ -95,6 +95,7 @@ __global__ void k_reset_pass(DevScalars *sc) {
     sc->walk_tiles = 0;
     sc->walk_decisions = 0;
     sc->walk_list = 0;
+    sc->walk_near = 0;
     sc->n_onodes = 0;
     sc->depth = 0;
     sc->max_stack = 0;

@@ -108,15 +108,29 @@ __device__ inline uint64_t descend_word(double x, double y, double z, double &cx
     return key;
 }
 
+// Two key words per particle: levels 1..21 (k1) and 22..42 (k2). Escaped
+// particles can make the root cube many orders of magnitude larger than the
+// bulk of the system, so the first 21 levels alone do not separate it.
 __global__ void k_keys(const double *__restrict__ pos, uint32_t n, const DevScalars *sc,
-                       uint64_t *__restrict__ key, uint32_t *__restrict__ idx) {
+                       uint64_t *__restrict__ k1_user, uint64_t *__restrict__ k2_sortkey,
+                       uint64_t *__restrict__ k2_user, uint32_t *__restrict__ idx) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double cx = sc->root_center[0], cy = sc->root_center[1], cz = sc->root_center[2];
     double side = sc->root_side;
-    key[i] = descend_word(pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2], cx, cy,
-                          cz, side);
+    const double x = pos[3 * (size_t)i], y = pos[3 * (size_t)i + 1], z = pos[3 * (size_t)i + 2];
+    const uint64_t a = descend_word(x, y, z, cx, cy, cz, side);
+    const uint64_t b = descend_word(x, y, z, cx, cy, cz, side);
+    k1_user[i] = a;
+    k2_sortkey[i] = b;
+    k2_user[i] = b;
     idx[i] = i;
+}
+
+__global__ void k_gather_key(const uint64_t *__restrict__ src, const uint32_t *__restrict__ idx,
+                             uint64_t *__restrict__ dst, uint32_t n) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) dst[j] = src[idx[j]];
 }
 
 // ---------------------------------------------------------------------------
@@ -270,55 +284,55 @@ __global__ void k_gather_bodies(const uint32_t *__restrict__ idx, const double *
     body[j] = make_double4(pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2], mass[i]);
 }
 
-// Groups of particles whose 21-level keys agree get two more key words
-// (levels 22..63) and are re-sorted among themselves. Identical keys over all
-// 63 levels mean coincident particles (the reference recurses without bound).
+// Groups of particles whose 42-level keys agree get a third key word (levels
+// 43..63) and are re-sorted among themselves. Identical keys over all 63
+// levels mean coincident particles (the reference recurses without bound).
 constexpr int kMaxDeepGroup = 64;
 
-__global__ void k_deep_groups(uint64_t *__restrict__ key1, uint64_t *__restrict__ key2,
+__global__ void k_deep_groups(const uint64_t *__restrict__ key1, const uint64_t *__restrict__ key2,
                               uint64_t *__restrict__ key3, uint32_t *__restrict__ idx,
                               double4 *__restrict__ body, uint32_t n, DevScalars *sc) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i + 1 >= n) return;
-    uint64_t k = key1[i];
-    if (key1[i + 1] != k) return;
-    if (i > 0 && key1[i - 1] == k) return;  // not the first of its group
+    const uint64_t k = key1[i], kk = key2[i];
+    if (key1[i + 1] != k || key2[i + 1] != kk) return;
+    if (i > 0 && key1[i - 1] == k && key2[i - 1] == kk) return;  // not the first of its group
     uint32_t e = i + 1;
-    while (e + 1 < n && key1[e + 1] == k) e++;
-    uint32_t g = e - i + 1;
+    while (e + 1 < n && key1[e + 1] == k && key2[e + 1] == kk) e++;
+    const uint32_t g = e - i + 1;
     atomicAdd(&sc->deep_groups, 1u);
     atomicOr(&sc->status, kStatusDeepGroup);
     if (g > kMaxDeepGroup) {
-        // Too many particles in one cell of side 2^-21 of the root: reported as
-        // coincident. Zero deep keys keep the radix tree well formed (ties
-        // then break on sorted position).
-        for (uint32_t j = i; j <= e; j++) key2[j] = key3[j] = 0;
+        // More than 64 particles inside one cell of side 2^-42 of the root:
+        // reported as coincident. Zero third words keep the radix tree well
+        // formed (ties then break on sorted position).
+        for (uint32_t j = i; j <= e; j++) key3[j] = 0;
         atomicOr(&sc->status, kStatusCoincident);
         return;
     }
     const double rcx = sc->root_center[0], rcy = sc->root_center[1], rcz = sc->root_center[2];
     const double rs = sc->root_side;
     for (uint32_t j = i; j <= e; j++) {
-        double4 b = body[j];
+        const double4 b = body[j];
         double cx = rcx, cy = rcy, cz = rcz, s = rs;
         descend_word(b.x, b.y, b.z, cx, cy, cz, s);
-        key2[j] = descend_word(b.x, b.y, b.z, cx, cy, cz, s);
+        descend_word(b.x, b.y, b.z, cx, cy, cz, s);
         key3[j] = descend_word(b.x, b.y, b.z, cx, cy, cz, s);
     }
-    // insertion sort of the group by (key2, key3)
+    // insertion sort of the group by its third word
     for (uint32_t j = i + 1; j <= e; j++) {
-        uint64_t a2 = key2[j], a3 = key3[j];
-        uint32_t ai = idx[j];
-        double4 ab = body[j];
+        const uint64_t a3 = key3[j];
+        const uint32_t ai = idx[j];
+        const double4 ab = body[j];
         uint32_t p = j;
-        while (p > i && (key2[p - 1] > a2 || (key2[p - 1] == a2 && key3[p - 1] > a3))) {
-            key2[p] = key2[p - 1]; key3[p] = key3[p - 1]; idx[p] = idx[p - 1]; body[p] = body[p - 1];
+        while (p > i && key3[p - 1] > a3) {
+            key3[p] = key3[p - 1]; idx[p] = idx[p - 1]; body[p] = body[p - 1];
             p--;
         }
-        key2[p] = a2; key3[p] = a3; idx[p] = ai; body[p] = ab;
+        key3[p] = a3; idx[p] = ai; body[p] = ab;
     }
     for (uint32_t j = i; j < e; j++)
-        if (key2[j] == key2[j + 1] && key3[j] == key3[j + 1]) atomicOr(&sc->status, kStatusCoincident);
+        if (key3[j] == key3[j + 1]) atomicOr(&sc->status, kStatusCoincident);
 }
 
 // ---------------------------------------------------------------------------
@@ -520,28 +534,32 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
     if (n == 0) return cudaSuccess;
     // root cube (+ max |v| when requested)
     k_bbox<<<tb.bbox_blocks, 256, 0, st>>>(tb.pos, tb.vel_for_max, tb.mass, n, tb.bbox_partial, tb.sc);
-    k_keys<<<blocks_for(n, 256), 256, 0, st>>>(tb.pos, n, tb.sc, tb.key_a, tb.idx_a);
+    // keys: k1 (user order) -> key3, k2 -> key_a (sort key) and key2 (user order)
+    k_keys<<<blocks_for(n, 256), 256, 0, st>>>(tb.pos, n, tb.sc, tb.key3, tb.key_a, tb.key2, tb.idx_a);
     L += 2;
-    // radix sort over the 63 key bits
-    uint64_t *kin = tb.key_a, *kout = tb.key_b;
-    uint32_t *iin = tb.idx_a, *iout = tb.idx_b;
+    // LSD radix sort by (k1, k2): 8 passes on k2, then 8 passes on k1.
     const uint32_t nb = blocks_for(n, kSortTile);
-    for (int shift = 0; shift < 64; shift += 8) {
-        k_sort_hist<<<nb, kSortThreads, 0, st>>>(kin, n, shift, tb.sort_hist, nb);
-        L += 2 + scan_exclusive(tb.sort_hist, 256u * nb, tb.scan_tmp, nullptr, st);
-        k_sort_scatter<<<nb, kSortThreads, 0, st>>>(kin, iin, kout, iout, n, shift, tb.sort_hist, nb);
-        uint64_t *tk = kin; kin = kout; kout = tk;
-        uint32_t *ti = iin; iin = iout; iout = ti;
-    }
-    // 8 passes: the sorted data is back in key_a / idx_a
+    auto passes = [&](uint64_t *kin, uint64_t *kout, uint32_t *iin, uint32_t *iout) {
+        for (int shift = 0; shift < 64; shift += 8) {
+            k_sort_hist<<<nb, kSortThreads, 0, st>>>(kin, n, shift, tb.sort_hist, nb);
+            L += 2 + scan_exclusive(tb.sort_hist, 256u * nb, tb.scan_tmp, nullptr, st);
+            k_sort_scatter<<<nb, kSortThreads, 0, st>>>(kin, iin, kout, iout, n, shift, tb.sort_hist, nb);
+            uint64_t *tk = kin; kin = kout; kout = tk;
+            uint32_t *ti = iin; iin = iout; iout = ti;
+        }
+    };
+    passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b);          // result: key_a, idx_a
+    k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key3, tb.idx_a, tb.key_b, n);  // k1 in that order
+    passes(tb.key_b, tb.key_a, tb.idx_a, tb.idx_b);          // result: key_b (k1 sorted), idx_a
+    k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key2, tb.idx_a, tb.key_a, n);  // k2 sorted
     k_gather_bodies<<<blocks_for(n, 256), 256, 0, st>>>(tb.idx_a, tb.pos, tb.mass, tb.body, n);
-    L += 1;
+    L += 3;
     *launches += L;
     if (n < 2) return cudaGetLastError();
     L = 0;
-    k_deep_groups<<<blocks_for(n, 256), 256, 0, st>>>(tb.key_a, tb.key2, tb.key3, tb.idx_a, tb.body, n,
+    k_deep_groups<<<blocks_for(n, 256), 256, 0, st>>>(tb.key_b, tb.key_a, tb.key3, tb.idx_a, tb.body, n,
                                                        tb.sc);
-    KeyView kv{tb.key_a, tb.key2, tb.key3, (int)n};
+    KeyView kv{tb.key_b, tb.key_a, tb.key3, (int)n};
     const uint32_t m = n - 1;
     k_radix_tree<<<blocks_for(m, 256), 256, 0, st>>>(kv, tb.bleft, tb.bright, tb.bparent, tb.leaf_bparent,
                                                       tb.bdelta);

@@ -55,6 +55,8 @@ struct WarpSmem<false> {
     int child[32][8];
     float4 lc[kListCap];      // (com - ref).xyz, G m
     uint32_t lm[kListCap];
+    double4 nc[32];           // near list: com.xyz (absolute), G m
+    uint32_t nm[32];
 };
 
 template <>
@@ -127,6 +129,32 @@ __device__ inline void force_list_f32(const float4 *lc, const uint32_t *lm, int 
     }
 }
 
+// Bodies too close to the group's box for FP32 offsets: each lane forms its
+// offset in FP64 from absolute coordinates, then runs the FP32 pair force.
+template <bool kDamp, bool kPot>
+__device__ inline void force_near_f32(const double4 *nc, const uint32_t *nm, int count, int lane, double bx,
+                                      double by, double bz, float &ax, float &ay, float &az, float &pot,
+                                      uint32_t &cnt) {
+    for (int k = 0; k < count; k++) {
+        if (!((nm[k] >> lane) & 1u)) continue;
+        const double4 c = nc[k];
+        const float dx = (float)(c.x - bx), dy = (float)(c.y - by), dz = (float)(c.z - bz);
+        const float gm = (float)c.w;
+        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+        const float inv = rsqrtf(r2);
+        float f;
+        if constexpr (kDamp) {
+            const float r = r2 * inv;
+            f = gm * inv / (r2 + expf(-r));
+        } else {
+            f = gm * inv * (inv * inv);
+        }
+        ax = fmaf(f, dx, ax); ay = fmaf(f, dy, ay); az = fmaf(f, dz, az);
+        if constexpr (kPot) pot = fmaf(gm, inv, pot);
+        cnt++;
+    }
+}
+
 template <bool kDamp, bool kPot>
 __device__ inline void force_list_f64(const double4 *lc, const uint32_t *lm, int count, int lane, double bx,
                                       double by, double bz, double &ax, double &ay, double &az, double &pot,
@@ -189,6 +217,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
         const float pm_g = warp_maxf(fmaxf(fabsf(px), fmaxf(fabsf(py), fabsf(pz))));
         const float pm_tol = kTolPm * pm_g;
         const float tiny = (kTiny * pm_g) * (kTiny * pm_g);
+        const float near_r2 = (pm_g * 0x1p-9f) * (pm_g * 0x1p-9f);
         // Group bounding box of the offsets (lanes past n repeat lane 0): FP32
         // for the MIXED form, FP64 for the FP64 form (group-level test only).
         float lox = 0.f, hix = 0.f, loy = 0.f, hiy = 0.f, loz = 0.f, hiz = 0.f;
@@ -206,7 +235,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
 
         float fax = 0.f, fay = 0.f, faz = 0.f, fpot = 0.f;
         double dax = 0.0, day = 0.0, daz = 0.0, dpot = 0.0;
-        uint32_t cnt = 0, nfallback = 0, nentries = 0, ntiles = 0, ndecide = 0, nlist = 0;
+        uint32_t cnt = 0, nfallback = 0, nentries = 0, ntiles = 0, ndecide = 0, nlist = 0, nnear = 0;
         int top = 0, list_top = 0, max_top = 0;
         uint32_t spill_top = 0;
         bool failed = false;
@@ -350,10 +379,21 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
                 }
             }
 
-            // ---- accepted bodies -> interaction list (compacted across lanes)
+            // ---- accepted bodies -> interaction list (compacted across lanes).
+            // MIXED: a body closer to the group's box than 2^-9 of the group's
+            // extent would lose too many bits in FP32 offsets (and could give a
+            // zero r^2); it goes to the near list, whose offsets are taken in FP64.
             const uint32_t accm = reach & ~my_open;
-            const uint32_t am = __ballot_sync(FULL, accm != 0);
-            if (accm) {
+            bool near = false;
+            if constexpr (!kFp64) {
+                if (accm) {
+                    const float ax_ = fmaxf(fmaxf(lox - fcx, fcx - hix), 0.f), ay_ = fmaxf(fmaxf(loy - fcy, fcy - hiy), 0.f),
+                                az_ = fmaxf(fmaxf(loz - fcz, fcz - hiz), 0.f);
+                    near = fmaf(az_, az_, fmaf(ay_, ay_, ax_ * ax_)) < near_r2;
+                }
+            }
+            const uint32_t am = __ballot_sync(FULL, accm != 0 && !near);
+            if (accm && !near) {
                 const int pos = list_top + __popc(am & lt);
                 if constexpr (kFp64) s.lc[pos] = make_double4(cx, cy, cz, kG * m);
                 else s.lc[pos] = make_float4(fcx, fcy, fcz, (float)(kG * m));
@@ -361,6 +401,20 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
             }
             list_top += __popc(am);
             nlist += __popc(am);
+            if constexpr (!kFp64) {
+                const uint32_t nmk = __ballot_sync(FULL, near);
+                if (nmk) {
+                    if (near) {
+                        const int pos = __popc(nmk & lt);
+                        s.nc[pos] = make_double4(cx, cy, cz, kG * m);
+                        s.nm[pos] = accm;
+                    }
+                    __syncwarp();
+                    force_near_f32<kDamp, kPot>(s.nc, s.nm, __popc(nmk), lane, b.x, b.y, b.z, fax, fay, faz, fpot, cnt);
+                    nnear += __popc(nmk);
+                    __syncwarp();
+                }
+            }
 
             // ---- children of opened nodes -> stack
             const int myn = my_open ? nch : 0;
@@ -429,6 +483,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
             atomicAdd(&t.sc->walk_tiles, (unsigned long long)ntiles);
             atomicAdd(&t.sc->walk_decisions, (unsigned long long)ndecide);
             atomicAdd(&t.sc->walk_list, (unsigned long long)nlist);
+            if (nnear) atomicAdd(&t.sc->walk_near, (unsigned long long)nnear);
             atomicMax(&t.sc->max_stack, (uint32_t)max_top);
             if (a.track_max_acc) atomic_max_nonneg(&t.sc->max_acc_bits, amag);
         }

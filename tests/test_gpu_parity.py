@@ -110,6 +110,22 @@ def test_close_pairs_need_deep_keys(nb, eng, eng64, orc):
     assert np.array_equal(cnt, rc)
 
 
+def test_escaped_particles_need_two_key_words(nb, eng, eng64, orc):
+    """Far escapees blow the root cube up by ~1e7: the bulk then shares its first
+    21 octree levels, and separating it needs the second key word."""
+    pos, _, mass = nb.generate(6000, seed=11)
+    pos[0] = [3.0e9, -1.0e9, 2.0e9]
+    pos[1] = [-2.5e9, 2.0e9, -3.0e9]
+    ra, rc = orc.forces(pos, mass, 0.5)
+    acc, cnt = eng64.barnes_hut(pos, mass, counts=True)
+    assert np.array_equal(cnt, rc)
+    assert rel(acc, ra).max() <= 1e-9
+    acc, cnt = eng.barnes_hut(pos, mass, counts=True)
+    assert np.array_equal(cnt, rc)
+    assert np.percentile(rel(acc, ra), 99) <= P99_MIXED
+    assert eng.stats()["tree_depth"] > 21
+
+
 def test_coincident_particles_rejected(nb, eng):
     pos, _, mass = nb.generate(100)
     pos[7] = pos[3]
