@@ -255,6 +255,10 @@ int ref_run_frames(unsigned int n, double *pos, double *vel, const double *mass,
     return 0;
 }
 
+/* The reference's unmodified main() (src/main.cpp:1359-1504), for running the
+ * whole program in-process: argv[1] is a settings file; output goes to ./data. */
+int ref_main(int argc, char **argv) { return nbodysim_reference_main(argc, argv); }
+
 /* Branching nodes of the reference tree (nodes with >= 2 non-empty children,
  * plus the root), pre-order. Each record: level, particle count, smallest
  * input index inside, mass, com, side. Returns the record count (or the
