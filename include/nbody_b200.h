@@ -151,6 +151,27 @@ typedef struct nbody_diagnostics {
  * extra force pass with potentials. */
 int nbody_get_diagnostics(nbody_ctx *ctx, nbody_diagnostics *out);
 
+/* ---- differentiation ----------------------------------------------------
+ * Reverse mode through the Barnes-Hut step with every step's opening decisions
+ * and interaction lists frozen (no reference counterpart). Pair terms follow
+ * the pair force's Jacobian; node terms flow through each node's centre of
+ * mass and total mass to every particle inside it. */
+
+/* Vector-Jacobian product of one force pass at the given state (host arrays):
+ * dL_dpos = (da/dx)^T dL_dacc and dL_dmass = (da/dm)^T dL_dacc, n x 3 and n. */
+int nbody_force_vjp(nbody_ctx *ctx, uint32_t n, const double *pos, const double *mass, const double *dL_dacc,
+                    double *dL_dpos, double *dL_dmass);
+/* nsteps fixed-dt steps from the resident state, keeping (pos, vel) every
+ * `checkpoint_every` steps (0: ceil(sqrt(nsteps))). The state at nsteps stays
+ * resident. Needs adaptive = 0. */
+int nbody_forward_checkpointed(nbody_ctx *ctx, uint32_t nsteps, uint32_t checkpoint_every);
+/* Reverse pass of the last nbody_forward_checkpointed: given dL/dpos and
+ * dL/dvel at the final step (host n x 3; dL_dvel may be NULL for zero), writes
+ * dL/dpos0, dL/dvel0 (n x 3) and dL/dmass (n) at the initial step. Segments
+ * between checkpoints are recomputed forward, bit-identically. */
+int nbody_backward(nbody_ctx *ctx, const double *dL_dpos, const double *dL_dvel, double *dL_dpos0,
+                   double *dL_dvel0, double *dL_dmass);
+
 /* ---- initial conditions ----------------------------------------------
  * Seeded generator of src/main.cpp:184-275 (std::default_random_engine, the
  * same draw order), so a seed gives the reference's particles bit for bit. */

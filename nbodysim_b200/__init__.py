@@ -117,6 +117,10 @@ _SIGS = {
     "nbody_generate": (C.c_int, [C.POINTER(GenParams), C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "nbody_status_string": (C.c_char_p, [C.c_int]),
     "nbody_last_error_message": (C.c_char_p, []),
+    "nbody_force_vjp": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p]),
+    "nbody_forward_checkpointed": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32]),
+    "nbody_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "nbody_probe_fp32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "nbody_root_cube_noalloc_max_n": (C.c_uint32, []),
     "nbody_root_cube_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
@@ -289,6 +293,29 @@ class Engine:
         _check(self._lib.nbody_step_host(self._h, n, pos.ctypes.data, vel.ctypes.data, mass.ctypes.data, nsteps))
         self.n = n
         return pos, vel
+
+    def force_vjp(self, pos, mass, dL_dacc):
+        """(dL/dpos, dL/dmass) of one force pass with frozen opening decisions."""
+        pos = _aos(pos)
+        n = pos.shape[0]
+        mass = _vec(mass, n)
+        la = _aos(dL_dacc, n)
+        gp = np.zeros((n, 3)); gm = np.zeros(n)
+        _check(self._lib.nbody_force_vjp(self._h, n, pos.ctypes.data, mass.ctypes.data, la.ctypes.data,
+                                         gp.ctypes.data, gm.ctypes.data))
+        return gp, gm
+
+    def forward_checkpointed(self, nsteps: int, every: int = 0) -> None:
+        _check(self._lib.nbody_forward_checkpointed(self._h, nsteps, every))
+
+    def backward(self, dL_dpos, dL_dvel=None):
+        """(dL/dpos0, dL/dvel0, dL/dmass) of the last forward_checkpointed."""
+        gp = _aos(dL_dpos, self.n)
+        gv = _aos(dL_dvel, self.n) if dL_dvel is not None else None
+        p0 = np.zeros((self.n, 3)); v0 = np.zeros((self.n, 3)); m0 = np.zeros(self.n)
+        _check(self._lib.nbody_backward(self._h, gp.ctypes.data, _ptr(gv), p0.ctypes.data, v0.ctypes.data,
+                                        m0.ctypes.data))
+        return p0, v0, m0
 
     def stats(self) -> dict:
         s = Stats()

@@ -72,6 +72,14 @@ struct nbody_ctx {
     cudaEvent_t ev[5] = {};
     nbody_stats stats{};
     unsigned long long launches = 0;  // kernels enqueued by this context
+    // adjoint state (allocated on first use)
+    void *adj_arena = nullptr;
+    size_t adj_bytes = 0;
+    double *lx = nullptr, *lv = nullptr, *lm = nullptr, *lam = nullptr, *gdir = nullptr;
+    double *adj_node = nullptr, *adj_leaf = nullptr, *vel_work = nullptr, *seg_pos = nullptr, *ckpt = nullptr;
+    uint32_t fwd_steps = 0, fwd_every = 0, fwd_n = 0;
+    double fwd_dt = 0.0;
+    bool have_fwd = false;
 };
 
 namespace {
@@ -196,11 +204,12 @@ void ev(nbody_ctx *c, int k) {
 
 // One force pass on the resident pos/mass: tree, COM, walk. Asynchronous.
 int force_pass(nbody_ctx *c, int damping, double theta, bool fp64, bool want_vmax, bool track_amax,
-               bool want_counts, bool want_pot) {
+               bool want_counts, bool want_pot, const double *pos = nullptr, bool adjoint = false) {
     const uint32_t n = c->n;
     unsigned launches = 1;
     NB_CUDA(launch_reset_pass(c->sc, c->stream));
     tree_inputs(c, n, want_vmax);
+    if (pos) c->tb.pos = pos;
     ev(c, 0);
     NB_CUDA(build_octree(c->tb, c->stream, &launches));
     ev(c, 1);
@@ -224,6 +233,17 @@ int force_pass(nbody_ctx *c, int damping, double theta, bool fp64, bool want_vma
     a.spill_cap = kSpillCap;
     a.n_groups = (n + 31) / 32;
     a.track_max_acc = track_amax ? 1 : 0;
+    if (adjoint) {
+        a.adjoint = 1;
+        a.lamf = (const float *)c->lam;
+        a.lamd = c->lam;
+        a.gdirf = (float *)c->gdir;
+        a.gdird = c->gdir;
+        a.adj_node = c->adj_node;
+        a.adj_leaf = c->adj_leaf;
+        NB_CUDA(cudaMemsetAsync(c->adj_node, 0, 32 * (size_t)n, c->stream));
+        NB_CUDA(cudaMemsetAsync(c->adj_leaf, 0, 32 * (size_t)n, c->stream));
+    }
     if (n > 0) {
         NB_CUDA(launch_walk(a, fp64, fp64 ? c->wl_fp64 : c->wl_mixed, c->stream));
         launches++;
@@ -282,6 +302,61 @@ int run_steps(nbody_ctx *c, uint32_t nsteps) {
         c->launches++;
         ev(c, 4);
     }
+    return NBODY_OK;
+}
+
+// Adjoint buffers for n particles, `seg` positions per checkpoint segment and
+// `nckpt` checkpoints of (pos, vel).
+int reserve_adjoint(nbody_ctx *c, uint32_t n, uint32_t seg, uint32_t nckpt) {
+    const size_t N = n;
+    struct Piece { double **dst; size_t bytes; };
+    Piece pieces[] = {
+        {&c->lx, 24 * N}, {&c->lv, 24 * N}, {&c->lm, 8 * N}, {&c->lam, 24 * N}, {&c->gdir, 24 * N},
+        {&c->adj_node, 32 * N}, {&c->adj_leaf, 32 * N}, {&c->vel_work, 24 * N},
+        {&c->seg_pos, 24 * N * seg}, {&c->ckpt, 48 * N * nckpt},
+    };
+    size_t total = 0;
+    for (auto &pc : pieces) total += align256(pc.bytes);
+    if (total > c->adj_bytes) {
+        NB_CUDA(cudaStreamSynchronize(c->stream));
+        if (c->adj_arena) NB_CUDA(cudaFree(c->adj_arena));
+        c->adj_arena = nullptr;
+        c->adj_bytes = 0;
+        cudaError_t e = cudaMalloc(&c->adj_arena, total);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            c->adj_arena = nullptr;
+            return fail(NBODY_ERR_OOM, "adjoint buffers (%s)", cudaGetErrorString(e));
+        }
+        c->adj_bytes = total;
+    }
+    char *p = (char *)c->adj_arena;
+    for (auto &pc : pieces) {
+        *pc.dst = (double *)p;
+        p += align256(pc.bytes);
+    }
+    return NBODY_OK;
+}
+
+// One reverse force step at positions `pos` with cotangent c->lam (dL/da):
+// tree and COM at pos, the adjoint walk over the same decisions, then the node
+// cotangents distributed to particles; adds into c->lx and c->lm.
+int adjoint_force(nbody_ctx *c, const double *pos, int damping, double theta, bool fp64) {
+    int rc = force_pass(c, damping, theta, fp64, false, false, false, false, pos, true);
+    if (rc) return rc;
+    NB_CUDA(launch_adj_distribute(c->tb.body, c->tb.idx_a, c->tb.leaf_oparent, c->tb.oparent, c->tb.onode,
+                                  c->adj_node, c->adj_leaf, c->gdir, fp64, c->lx, c->lm, c->n, c->stream));
+    c->launches++;
+    return NBODY_OK;
+}
+
+// One forward step on explicit buffers (recomputation inside a segment).
+int step_on(nbody_ctx *c, double *pos, double *vel, bool fp64) {
+    StepParams sp{c->p.dt, 0, 0, 0, 0};
+    int rc = force_pass(c, c->p.damping, c->p.theta, fp64, false, false, false, false, pos, false);
+    if (rc) return rc;
+    NB_CUDA(launch_update(pos, vel, c->acc, fp64, c->n, sp, c->sc, c->stream));
+    c->launches++;
     return NBODY_OK;
 }
 
@@ -351,6 +426,7 @@ int nbody_destroy(nbody_ctx *c) {
     cudaSetDevice(c->p.device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->arena) cudaFree(c->arena);
+    if (c->adj_arena) cudaFree(c->adj_arena);
     if (c->sc) cudaFree(c->sc);
     if (c->hsc) cudaFreeHost(c->hsc);
     for (auto &e : c->ev)
@@ -516,6 +592,112 @@ int nbody_get_diagnostics(nbody_ctx *c, nbody_diagnostics *out) {
     }
     out->mass = d[8];
     return NBODY_OK;
+}
+
+int nbody_force_vjp(nbody_ctx *c, uint32_t n, const double *pos, const double *mass, const double *dL_dacc,
+                    double *dL_dpos, double *dL_dmass) {
+    CTX_OR_FAIL(c);
+    if (n > kMaxParticles) return fail(NBODY_ERR_INVALID, "n exceeds the 2^28 particle limit%s");
+    if (n && (!pos || !mass || !dL_dacc || !dL_dpos || !dL_dmass)) return fail(NBODY_ERR_INVALID, "null array%s");
+    if (n == 0) return NBODY_OK;
+    int rc = upload(c, n, pos, nullptr, mass);
+    if (rc) return rc;
+    if ((rc = reserve_adjoint(c, n, 1, 0))) return rc;
+    if ((rc = begin_call(c))) return rc;
+    const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
+    NB_CUDA(cudaMemcpyAsync(c->lx, dL_dacc, 24 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    if (fp64) {
+        NB_CUDA(cudaMemcpyAsync(c->lam, c->lx, 24 * (size_t)n, cudaMemcpyDeviceToDevice, c->stream));
+    } else {
+        NB_CUDA(launch_double_to_float(c->lx, (float *)c->lam, 3 * (size_t)n, c->stream));
+        c->launches++;
+    }
+    NB_CUDA(cudaMemsetAsync(c->lx, 0, 24 * (size_t)n, c->stream));
+    NB_CUDA(cudaMemsetAsync(c->lm, 0, 8 * (size_t)n, c->stream));
+    if ((rc = adjoint_force(c, c->pos, c->p.damping, c->p.theta, fp64))) return rc;
+    NB_CUDA(cudaMemcpyAsync(dL_dpos, c->lx, 24 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    NB_CUDA(cudaMemcpyAsync(dL_dmass, c->lm, 8 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = copy_scalars_back(c))) return rc;
+    return check_status(c);
+}
+
+int nbody_forward_checkpointed(nbody_ctx *c, uint32_t nsteps, uint32_t every) {
+    CTX_OR_FAIL(c);
+    if (!c->have_state || !c->have_vel) return fail(NBODY_ERR_STATE, "particles with velocities must be set first%s");
+    if (c->p.adaptive) return fail(NBODY_ERR_INVALID, "the adjoint needs a fixed dt (adaptive = 0)%s");
+    c->have_fwd = false;
+    if (nsteps == 0 || c->n == 0) return NBODY_OK;
+    if (every == 0) {
+        every = 1;
+        while ((uint64_t)every * every < nsteps) every++;
+    }
+    if (every > nsteps) every = nsteps;
+    const uint32_t nseg = (nsteps + every - 1) / every;
+    int rc = reserve_adjoint(c, c->n, every, nseg);
+    if (rc) return rc;
+    if ((rc = begin_call(c))) return rc;
+    const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
+    const size_t N3 = 3 * (size_t)c->n;
+    for (uint32_t k = 0; k < nsteps; k++) {
+        if (k % every == 0) {
+            double *ck = c->ckpt + 2 * N3 * (k / every);
+            NB_CUDA(cudaMemcpyAsync(ck, c->pos, 8 * N3, cudaMemcpyDeviceToDevice, c->stream));
+            NB_CUDA(cudaMemcpyAsync(ck + N3, c->vel, 8 * N3, cudaMemcpyDeviceToDevice, c->stream));
+        }
+        if ((rc = step_on(c, c->pos, c->vel, fp64))) return rc;
+    }
+    if ((rc = copy_scalars_back(c))) return rc;
+    if ((rc = check_status(c))) return rc;
+    c->fwd_steps = nsteps;
+    c->fwd_every = every;
+    c->fwd_n = c->n;
+    c->fwd_dt = c->p.dt;
+    c->have_fwd = true;
+    return NBODY_OK;
+}
+
+int nbody_backward(nbody_ctx *c, const double *dL_dpos, const double *dL_dvel, double *dL_dpos0, double *dL_dvel0,
+                   double *dL_dmass) {
+    CTX_OR_FAIL(c);
+    if (!c->have_fwd || c->fwd_n != c->n) return fail(NBODY_ERR_STATE, "call nbody_forward_checkpointed first%s");
+    if (!dL_dpos || !dL_dpos0 || !dL_dvel0 || !dL_dmass) return fail(NBODY_ERR_INVALID, "null array%s");
+    const uint32_t n = c->n, K = c->fwd_steps, C = c->fwd_every;
+    const size_t N3 = 3 * (size_t)n;
+    const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
+    if (c->p.dt != c->fwd_dt) return fail(NBODY_ERR_STATE, "dt changed since the forward pass%s");
+    int rc = begin_call(c);
+    if (rc) return rc;
+    NB_CUDA(cudaMemcpyAsync(c->lx, dL_dpos, 8 * N3, cudaMemcpyHostToDevice, c->stream));
+    if (dL_dvel) NB_CUDA(cudaMemcpyAsync(c->lv, dL_dvel, 8 * N3, cudaMemcpyHostToDevice, c->stream));
+    else NB_CUDA(cudaMemsetAsync(c->lv, 0, 8 * N3, c->stream));
+    NB_CUDA(cudaMemsetAsync(c->lm, 0, 8 * (size_t)n, c->stream));
+    const uint32_t nseg = (K + C - 1) / C;
+    for (int seg = (int)nseg - 1; seg >= 0; seg--) {
+        const uint32_t k0 = (uint32_t)seg * C, len = (K - k0 < C) ? K - k0 : C;
+        const double *ck = c->ckpt + 2 * N3 * (size_t)seg;
+        NB_CUDA(cudaMemcpyAsync(c->seg_pos, ck, 8 * N3, cudaMemcpyDeviceToDevice, c->stream));
+        NB_CUDA(cudaMemcpyAsync(c->vel_work, ck + N3, 8 * N3, cudaMemcpyDeviceToDevice, c->stream));
+        for (uint32_t i = 0; i + 1 < len; i++) {
+            double *xi = c->seg_pos + N3 * i, *xn = xi + N3;
+            NB_CUDA(cudaMemcpyAsync(xn, xi, 8 * N3, cudaMemcpyDeviceToDevice, c->stream));
+            // forces at xi, then update the copy in place: x_{k+1}, v_{k+1}
+            rc = force_pass(c, c->p.damping, c->p.theta, fp64, false, false, false, false, xi, false);
+            if (rc) return rc;
+            StepParams sp{c->p.dt, 0, 0, 0, 0};
+            NB_CUDA(launch_update(xn, c->vel_work, c->acc, fp64, n, sp, c->sc, c->stream));
+            c->launches++;
+        }
+        for (int i = (int)len - 1; i >= 0; i--) {
+            NB_CUDA(launch_adj_pre(c->lx, c->lv, c->lam, fp64, c->p.dt, n, c->stream));
+            c->launches++;
+            if ((rc = adjoint_force(c, c->seg_pos + N3 * (size_t)i, c->p.damping, c->p.theta, fp64))) return rc;
+        }
+    }
+    NB_CUDA(cudaMemcpyAsync(dL_dpos0, c->lx, 8 * N3, cudaMemcpyDeviceToHost, c->stream));
+    NB_CUDA(cudaMemcpyAsync(dL_dvel0, c->lv, 8 * N3, cudaMemcpyDeviceToHost, c->stream));
+    NB_CUDA(cudaMemcpyAsync(dL_dmass, c->lm, 8 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = copy_scalars_back(c))) return rc;
+    return check_status(c);
 }
 
 const char *nbody_status_string(int s) {

@@ -112,6 +112,86 @@ __global__ void k_acc_to_double(const float *__restrict__ in, double *__restrict
     if (i < count) out[i] = (double)in[i];
 }
 
+// ---- adjoint -----------------------------------------------------------------
+// Reverse of particle::update (src/particle.cpp:66-74): with x' = x + v' dt and
+// v' = v + a dt, the cotangents of step k follow from those of step k+1 as
+//   mu = lv' + lx' dt;  lv = mu;  la = mu dt;  lx = lx' + (dF/dx)^T la.
+template <typename LT>
+__global__ void k_adj_pre(const double *__restrict__ lx, double *__restrict__ lv, LT *__restrict__ lam, double dt,
+                          uint32_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 3 * (size_t)n) return;
+    const double mu = lv[i] + lx[i] * dt;
+    lv[i] = mu;
+    lam[i] = (LT)(mu * dt);
+}
+
+// Node cotangents -> particles. A particle j inside node n (its own leaf and
+// every internal ancestor) receives (m_j / M_n) adj_c(n) in position, and
+// (x_j - c_n) . adj_c(n) / M_n + adj_M(n) in mass, from c_n = sum m x / M_n.
+template <typename GT>
+__global__ void k_adj_distribute(const double4 *__restrict__ body, const uint32_t *__restrict__ sidx,
+                                 const int32_t *__restrict__ leaf_oparent, const int32_t *__restrict__ oparent,
+                                 const double4 *__restrict__ onode, const double *__restrict__ adj_node,
+                                 const double *__restrict__ adj_leaf, const GT *__restrict__ gdir,
+                                 double *__restrict__ lx, double *__restrict__ lm, uint32_t n) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint32_t ui = sidx[j];
+    const double4 b = body[j];
+    double gx = (double)gdir[3 * (size_t)ui], gy = (double)gdir[3 * (size_t)ui + 1], gz = (double)gdir[3 * (size_t)ui + 2];
+    const double *al = adj_leaf + 4 * (size_t)j;
+    gx += al[0]; gy += al[1]; gz += al[2];
+    double gm = al[3];
+    int p = n > 1 ? leaf_oparent[j] : -1;
+    for (int hops = 0; p >= 0 && hops <= kMaxLevels + 1; hops++) {
+        const double4 nd = onode[p];
+        const double *an = adj_node + 4 * (size_t)p;
+        if (nd.w != 0.0) {
+            const double w = b.w / nd.w;
+            gx += w * an[0]; gy += w * an[1]; gz += w * an[2];
+            gm += ((b.x - nd.x) * an[0] + (b.y - nd.y) * an[1] + (b.z - nd.z) * an[2]) / nd.w;
+        }
+        gm += an[3];
+        p = oparent[p];
+    }
+    lx[3 * (size_t)ui] += gx; lx[3 * (size_t)ui + 1] += gy; lx[3 * (size_t)ui + 2] += gz;
+    lm[ui] += gm;
+}
+
+cudaError_t launch_adj_pre(const double *lx, double *lv, void *lam, bool lam_double, double dt, uint32_t n,
+                           cudaStream_t st) {
+    const unsigned blocks = (unsigned)((3 * (size_t)n + 255) / 256);
+    if (lam_double) k_adj_pre<double><<<blocks, 256, 0, st>>>(lx, lv, (double *)lam, dt, n);
+    else k_adj_pre<float><<<blocks, 256, 0, st>>>(lx, lv, (float *)lam, dt, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_distribute(const double4 *body, const uint32_t *sidx, const int32_t *leaf_oparent,
+                                  const int32_t *oparent, const double4 *onode, const double *adj_node,
+                                  const double *adj_leaf, const void *gdir, bool gdir_double, double *lx, double *lm,
+                                  uint32_t n, cudaStream_t st) {
+    const unsigned blocks = (n + 255) / 256;
+    if (gdir_double)
+        k_adj_distribute<double><<<blocks, 256, 0, st>>>(body, sidx, leaf_oparent, oparent, onode, adj_node, adj_leaf,
+                                                         (const double *)gdir, lx, lm, n);
+    else
+        k_adj_distribute<float><<<blocks, 256, 0, st>>>(body, sidx, leaf_oparent, oparent, onode, adj_node, adj_leaf,
+                                                        (const float *)gdir, lx, lm, n);
+    return cudaGetLastError();
+}
+
+__global__ void k_double_to_float(const double *__restrict__ in, float *__restrict__ out, size_t count) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) out[i] = (float)in[i];
+}
+
+cudaError_t launch_double_to_float(const double *in, float *out, size_t count, cudaStream_t st) {
+    if (!count) return cudaSuccess;
+    k_double_to_float<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(in, out, count);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_update(double *pos, double *vel, const void *acc, bool acc_double, uint32_t n,
                           const StepParams &sp, DevScalars *sc, cudaStream_t st) {
     const unsigned blocks = n ? (n + 255) / 256 : 1;

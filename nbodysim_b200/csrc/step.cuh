@@ -19,5 +19,12 @@ cudaError_t launch_diag(const double *pos, const double *vel, const double *mass
                         uint32_t n, double *partial, unsigned blocks, DevScalars *sc, cudaStream_t st);
 cudaError_t launch_reset_pass(DevScalars *sc, cudaStream_t st);
 cudaError_t launch_acc_to_double(const float *in, double *out, size_t count, cudaStream_t st);
+cudaError_t launch_double_to_float(const double *in, float *out, size_t count, cudaStream_t st);
+cudaError_t launch_adj_pre(const double *lx, double *lv, void *lam, bool lam_double, double dt, uint32_t n,
+                           cudaStream_t st);
+cudaError_t launch_adj_distribute(const double4 *body, const uint32_t *sidx, const int32_t *leaf_oparent,
+                                  const int32_t *oparent, const double4 *onode, const double *adj_node,
+                                  const double *adj_leaf, const void *gdir, bool gdir_double, double *lx, double *lm,
+                                  uint32_t n, cudaStream_t st);
 
 }  // namespace nbody

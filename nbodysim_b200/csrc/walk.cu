@@ -55,8 +55,10 @@ struct WarpSmem<false> {
     int child[32][8];
     float4 lc[kListCap];      // (com - ref).xyz, G m
     uint32_t lm[kListCap];
+    int lr[kListCap];         // node refs (adjoint mode)
     double4 nc[32];           // near list: com.xyz (absolute), G m
     uint32_t nm[32];
+    int nr[32];
 };
 
 template <>
@@ -67,6 +69,7 @@ struct WarpSmem<true> {
     int child[32][8];
     double4 lc[kListCap];     // com.xyz (absolute), G m
     uint32_t lm[kListCap];
+    int lr[kListCap];
 };
 
 // The reference's FP64 opening test on the original doubles
@@ -155,6 +158,124 @@ __device__ inline void force_near_f32(const double4 *nc, const uint32_t *nm, int
     }
 }
 
+// ---- adjoint pair terms (frozen decisions) --------------------------------
+// For a taken pair with offset d = com - x and cotangent la = dL/da_i:
+//   F = G M g(r) d,  dF/dd = G M (g I + h d d^T),  h = g'(r) / r,  dF/dM = G g d
+//   undamped g = r^-3, h = -3 r^-5; damped g = 1 / (r (r^2 + e^-r)).
+// v = (dF/dd) la goes to the node's centre-of-mass cotangent and, negated, to
+// the particle's own position; G g (d . la) goes to the node's mass cotangent.
+template <bool kDamp, typename T>
+__device__ inline void pair_adjoint(T dx, T dy, T dz, T r2, T gm, T lax, T lay, T laz, T &vx, T &vy, T &vz,
+                                    T &mterm) {
+    T inv, g, h;
+    if constexpr (sizeof(T) == 4) inv = rsqrtf(r2);
+    else inv = 1.0 / sqrt(r2);
+    const T inv2 = inv * inv;
+    if constexpr (kDamp) {
+        const T r = r2 * inv;
+        T e;
+        if constexpr (sizeof(T) == 4) e = expf(-r);
+        else e = exp(-r);
+        const T den = r2 + e;
+        g = inv / den;
+        h = -(T(3) * r2 + e - r * e) * inv2 * inv / (den * den);
+    } else {
+        g = inv * inv2;
+        h = T(-3) * g * inv2;
+    }
+    const T s = dx * lax + dy * lay + dz * laz;
+    const T hs = h * s;
+    vx = gm * (g * lax + hs * dx);
+    vy = gm * (g * lay + hs * dy);
+    vz = gm * (g * laz + hs * dz);
+    mterm = T(kG) * g * s;
+}
+
+// Sums four per-lane values over the warp in six shuffles; lane 0 ends with
+// the sum of a, lane 8 of b, lane 16 of c, lane 24 of d.
+template <typename T>
+__device__ inline T warp_sum4(T a, T b, T c, T d, int lane) {
+    const bool h16 = lane & 16;
+    T x0 = h16 ? c : a, x1 = h16 ? d : b;
+    const T y0 = h16 ? a : c, y1 = h16 ? b : d;
+    x0 += __shfl_xor_sync(0xffffffffu, y0, 16);
+    x1 += __shfl_xor_sync(0xffffffffu, y1, 16);
+    const bool h8 = lane & 8;
+    T z = h8 ? x1 : x0;
+    const T w = h8 ? x0 : x1;
+    z += __shfl_xor_sync(0xffffffffu, w, 8);
+    z += __shfl_xor_sync(0xffffffffu, z, 4);
+    z += __shfl_xor_sync(0xffffffffu, z, 2);
+    z += __shfl_xor_sync(0xffffffffu, z, 1);
+    return z;
+}
+
+__device__ inline void scatter_adj(double *adj_node, double *adj_leaf, int ref, double z, int lane) {
+    if ((lane & 7) == 0) {
+        double *dst = ref >= 0 ? adj_node + 4 * (size_t)ref : adj_leaf + 4 * (size_t)(~ref);
+        atomicAdd(dst + (lane >> 3), z);
+    }
+}
+
+template <bool kDamp>
+__device__ inline void adj_list_f32(const float4 *lc, const uint32_t *lm, const int *lr, int count, int lane,
+                                    float px, float py, float pz, float lax, float lay, float laz, float &gx,
+                                    float &gy, float &gz, double *adj_node, double *adj_leaf, uint32_t &cnt) {
+    for (int k = 0; k < count; k++) {
+        const float4 c = lc[k];
+        const bool take = (lm[k] >> lane) & 1u;
+        const float dx = c.x - px, dy = c.y - py, dz = c.z - pz;
+        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+        float vx, vy, vz, mt;
+        pair_adjoint<kDamp, float>(dx, dy, dz, r2, c.w, lax, lay, laz, vx, vy, vz, mt);
+        if (!take) vx = vy = vz = mt = 0.f;
+        else cnt++;
+        gx -= vx; gy -= vy; gz -= vz;
+        const float z = warp_sum4(vx, vy, vz, mt, lane);
+        scatter_adj(adj_node, adj_leaf, lr[k], (double)z, lane);
+    }
+}
+
+template <bool kDamp>
+__device__ inline void adj_near_f32(const double4 *nc, const uint32_t *nm, const int *nr, int count, int lane,
+                                    double bx, double by, double bz, float lax, float lay, float laz, float &gx,
+                                    float &gy, float &gz, double *adj_node, double *adj_leaf, uint32_t &cnt) {
+    for (int k = 0; k < count; k++) {
+        const double4 c = nc[k];
+        const bool take = (nm[k] >> lane) & 1u;
+        float vx = 0.f, vy = 0.f, vz = 0.f, mt = 0.f;
+        if (take) {
+            const float dx = (float)(c.x - bx), dy = (float)(c.y - by), dz = (float)(c.z - bz);
+            const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            pair_adjoint<kDamp, float>(dx, dy, dz, r2, (float)c.w, lax, lay, laz, vx, vy, vz, mt);
+            cnt++;
+        }
+        gx -= vx; gy -= vy; gz -= vz;
+        const float z = warp_sum4(vx, vy, vz, mt, lane);
+        scatter_adj(adj_node, adj_leaf, nr[k], (double)z, lane);
+    }
+}
+
+template <bool kDamp>
+__device__ inline void adj_list_f64(const double4 *lc, const uint32_t *lm, const int *lr, int count, int lane,
+                                    double bx, double by, double bz, double lax, double lay, double laz, double &gx,
+                                    double &gy, double &gz, double *adj_node, double *adj_leaf, uint32_t &cnt) {
+    for (int k = 0; k < count; k++) {
+        const double4 c = lc[k];
+        const bool take = (lm[k] >> lane) & 1u;
+        double vx = 0.0, vy = 0.0, vz = 0.0, mt = 0.0;
+        if (take) {
+            const double dx = c.x - bx, dy = c.y - by, dz = c.z - bz;
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            pair_adjoint<kDamp, double>(dx, dy, dz, r2, c.w, lax, lay, laz, vx, vy, vz, mt);
+            cnt++;
+        }
+        gx -= vx; gy -= vy; gz -= vz;
+        const double z = warp_sum4(vx, vy, vz, mt, lane);
+        scatter_adj(adj_node, adj_leaf, lr[k], z, lane);
+    }
+}
+
 template <bool kDamp, bool kPot>
 __device__ inline void force_list_f64(const double4 *lc, const uint32_t *lm, int count, int lane, double bx,
                                       double by, double bz, double &ax, double &ay, double &az, double &pot,
@@ -177,7 +298,24 @@ __device__ inline void force_list_f64(const double4 *lc, const uint32_t *lm, int
     }
 }
 
-template <bool kFp64, bool kDamp, bool kPot>
+template <bool kFp64, bool kDamp, bool kPot, bool kAdj, class Sm>
+__device__ inline void flush_list(Sm &s, int count, int lane, const WalkArgs &a, const double4 &b, float px, float py,
+                                  float pz, double lax, double lay, double laz, float &fax, float &fay, float &faz,
+                                  float &fpot, double &dax, double &day, double &daz, double &dpot, uint32_t &cnt) {
+    if constexpr (kAdj) {
+        if constexpr (kFp64)
+            adj_list_f64<kDamp>(s.lc, s.lm, s.lr, count, lane, b.x, b.y, b.z, lax, lay, laz, dax, day, daz, a.adj_node,
+                                a.adj_leaf, cnt);
+        else
+            adj_list_f32<kDamp>(s.lc, s.lm, s.lr, count, lane, px, py, pz, (float)lax, (float)lay, (float)laz, fax, fay,
+                                faz, a.adj_node, a.adj_leaf, cnt);
+    } else {
+        if constexpr (kFp64) force_list_f64<kDamp, kPot>(s.lc, s.lm, count, lane, b.x, b.y, b.z, dax, day, daz, dpot, cnt);
+        else force_list_f32<kDamp, kPot>(s.lc, s.lm, count, lane, px, py, pz, fax, fay, faz, fpot, cnt);
+    }
+}
+
+template <bool kFp64, bool kDamp, bool kPot, bool kAdj>
 __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using Sm = WarpSmem<kFp64>;
@@ -203,6 +341,15 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
         const bool valid = j < n;
         const double4 b = t.body[valid ? j : g0];
         const uint32_t vmask = __ballot_sync(FULL, valid);
+        // adjoint mode: this particle's cotangent dL/da
+        double lax = 0.0, lay = 0.0, laz = 0.0;
+        if constexpr (kAdj) {
+            if (valid) {
+                const size_t u3 = 3 * (size_t)t.sidx[j];
+                if constexpr (kFp64) { lax = a.lamd[u3]; lay = a.lamd[u3 + 1]; laz = a.lamd[u3 + 2]; }
+                else { lax = a.lamf[u3]; lay = a.lamf[u3 + 1]; laz = a.lamf[u3 + 2]; }
+            }
+        }
 
         // Reference point: centre of the group's bounding box.
         const double rx = 0.5 * (warp_min(b.x) + warp_max(b.x));
@@ -398,6 +545,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
                 if constexpr (kFp64) s.lc[pos] = make_double4(cx, cy, cz, kG * m);
                 else s.lc[pos] = make_float4(fcx, fcy, fcz, (float)(kG * m));
                 s.lm[pos] = accm;
+                s.lr[pos] = ref;
             }
             list_top += __popc(am);
             nlist += __popc(am);
@@ -408,9 +556,14 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
                         const int pos = __popc(nmk & lt);
                         s.nc[pos] = make_double4(cx, cy, cz, kG * m);
                         s.nm[pos] = accm;
+                        s.nr[pos] = ref;
                     }
                     __syncwarp();
-                    force_near_f32<kDamp, kPot>(s.nc, s.nm, __popc(nmk), lane, b.x, b.y, b.z, fax, fay, faz, fpot, cnt);
+                    if constexpr (kAdj)
+                        adj_near_f32<kDamp>(s.nc, s.nm, s.nr, __popc(nmk), lane, b.x, b.y, b.z, (float)lax, (float)lay,
+                                            (float)laz, fax, fay, faz, a.adj_node, a.adj_leaf, cnt);
+                    else
+                        force_near_f32<kDamp, kPot>(s.nc, s.nm, __popc(nmk), lane, b.x, b.y, b.z, fax, fay, faz, fpot, cnt);
                     nnear += __popc(nmk);
                     __syncwarp();
                 }
@@ -440,16 +593,16 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
 
             // ---- forces once the list is long enough
             if (list_top >= kListFlush) {
-                if constexpr (kFp64) force_list_f64<kDamp, kPot>(s.lc, s.lm, list_top, lane, b.x, b.y, b.z, dax, day, daz, dpot, cnt);
-                else force_list_f32<kDamp, kPot>(s.lc, s.lm, list_top, lane, px, py, pz, fax, fay, faz, fpot, cnt);
+                flush_list<kFp64, kDamp, kPot, kAdj>(s, list_top, lane, a, b, px, py, pz, lax, lay, laz, fax, fay, faz,
+                                                      fpot, dax, day, daz, dpot, cnt);
                 list_top = 0;
                 __syncwarp();
             }
         }
         if (failed && lane == 0) atomicOr(&t.sc->status, kStatusCapacity);
         if (list_top > 0) {
-            if constexpr (kFp64) force_list_f64<kDamp, kPot>(s.lc, s.lm, list_top, lane, b.x, b.y, b.z, dax, day, daz, dpot, cnt);
-            else force_list_f32<kDamp, kPot>(s.lc, s.lm, list_top, lane, px, py, pz, fax, fay, faz, fpot, cnt);
+            flush_list<kFp64, kDamp, kPot, kAdj>(s, list_top, lane, a, b, px, py, pz, lax, lay, laz, fax, fay, faz, fpot,
+                                                  dax, day, daz, dpot, cnt);
         }
         __syncwarp();
 
@@ -459,7 +612,13 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
         else { ax = fax; ay = fay; az = faz; }
         if (valid) {
             const uint32_t ui = t.sidx[j];
-            if constexpr (kFp64) {
+            if constexpr (kAdj) {
+                if constexpr (kFp64) {
+                    a.gdird[3 * (size_t)ui] = ax; a.gdird[3 * (size_t)ui + 1] = ay; a.gdird[3 * (size_t)ui + 2] = az;
+                } else {
+                    a.gdirf[3 * (size_t)ui] = fax; a.gdirf[3 * (size_t)ui + 1] = fay; a.gdirf[3 * (size_t)ui + 2] = faz;
+                }
+            } else if constexpr (kFp64) {
                 a.accd[3 * (size_t)ui] = ax; a.accd[3 * (size_t)ui + 1] = ay; a.accd[3 * (size_t)ui + 2] = az;
             } else {
                 a.accf[3 * (size_t)ui] = fax; a.accf[3 * (size_t)ui + 1] = fay; a.accf[3 * (size_t)ui + 2] = faz;
@@ -474,7 +633,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
         uint32_t wf = nfallback;
         for (int o = 16; o; o >>= 1) wf += __shfl_xor_sync(FULL, wf, o);
         double amag = valid ? sqrt(ax * ax + ay * ay + az * az) : 0.0;
-        if (a.track_max_acc) amag = warp_max(amag);
+        if (!kAdj && a.track_max_acc) amag = warp_max(amag);
         if (lane == 0) {
             atomicAdd(&t.sc->interactions, wc);
             atomicAdd(&t.sc->interactions_total, wc);
@@ -485,37 +644,43 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
             atomicAdd(&t.sc->walk_list, (unsigned long long)nlist);
             if (nnear) atomicAdd(&t.sc->walk_near, (unsigned long long)nnear);
             atomicMax(&t.sc->max_stack, (uint32_t)max_top);
-            if (a.track_max_acc) atomic_max_nonneg(&t.sc->max_acc_bits, amag);
+            if (!kAdj && a.track_max_acc) atomic_max_nonneg(&t.sc->max_acc_bits, amag);
         }
     }
 }
 
-template <bool kFp64>
+template <bool kFp64, bool kAdj>
 const void *walk_kernel(int damping, bool pot) {
-    if (damping) return pot ? (const void *)k_walk<kFp64, true, true> : (const void *)k_walk<kFp64, true, false>;
-    return pot ? (const void *)k_walk<kFp64, false, true> : (const void *)k_walk<kFp64, false, false>;
+    if constexpr (kAdj) {
+        return damping ? (const void *)k_walk<kFp64, true, false, true> : (const void *)k_walk<kFp64, false, false, true>;
+    } else {
+        if (damping)
+            return pot ? (const void *)k_walk<kFp64, true, true, false> : (const void *)k_walk<kFp64, true, false, false>;
+        return pot ? (const void *)k_walk<kFp64, false, true, false> : (const void *)k_walk<kFp64, false, false, false>;
+    }
+}
+
+const void *any_walk_kernel(bool fp64, bool adj, int damping, bool pot) {
+    if (fp64) return adj ? walk_kernel<true, true>(damping, pot) : walk_kernel<true, false>(damping, pot);
+    return adj ? walk_kernel<false, true>(damping, pot) : walk_kernel<false, false>(damping, pot);
 }
 
 }  // namespace
 
 cudaError_t walk_launch_shape(bool fp64, int device, WalkLaunch *out) {
     const size_t smem = (fp64 ? sizeof(WarpSmem<true>) : sizeof(WarpSmem<false>)) * kWalkWarps;
-    const void *kernels[8] = {
-        (const void *)k_walk<false, false, false>, (const void *)k_walk<false, false, true>,
-        (const void *)k_walk<false, true, false>, (const void *)k_walk<false, true, true>,
-        (const void *)k_walk<true, false, false>, (const void *)k_walk<true, false, true>,
-        (const void *)k_walk<true, true, false>, (const void *)k_walk<true, true, true>};
     int minblocks = 1 << 30;
-    for (int k = 0; k < 8; k++) {
-        cudaError_t e = cudaFuncSetAttribute(kernels[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
-    for (int k = fp64 ? 4 : 0; k < (fp64 ? 8 : 4); k++) {
-        int nb = 0;
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernels[k], kWalkWarps * 32, smem);
-        if (e != cudaSuccess) return e;
-        minblocks = nb < minblocks ? nb : minblocks;
-    }
+    for (int adj = 0; adj < 2; adj++)
+        for (int damp = 0; damp < 2; damp++)
+            for (int pot = 0; pot < 2 - adj; pot++) {
+                const void *k = any_walk_kernel(fp64, adj, damp, pot);
+                cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                if (e != cudaSuccess) return e;
+                int nb = 0;
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kWalkWarps * 32, smem);
+                if (e != cudaSuccess) return e;
+                minblocks = nb < minblocks ? nb : minblocks;
+            }
     int sms = 0;
     cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
@@ -526,8 +691,7 @@ cudaError_t walk_launch_shape(bool fp64, int device, WalkLaunch *out) {
 }
 
 cudaError_t launch_walk(const WalkArgs &a, bool fp64, const WalkLaunch &l, cudaStream_t st) {
-    const void *k = fp64 ? walk_kernel<true>(a.damping, a.pot != nullptr)
-                         : walk_kernel<false>(a.damping, a.pot != nullptr);
+    const void *k = any_walk_kernel(fp64, a.adjoint != 0, a.damping, a.pot != nullptr);
     unsigned blocks = l.blocks;
     const unsigned need = (a.n_groups + kWalkWarps - 1) / kWalkWarps;
     if (need < blocks) blocks = need ? need : 1;

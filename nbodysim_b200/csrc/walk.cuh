@@ -23,6 +23,18 @@ struct WalkArgs {
     uint32_t spill_cap;
     uint32_t n_groups;  // ceil(n / 32)
     int track_max_acc;  // reduce max |a| (adaptive dt)
+    // Adjoint mode (frozen decisions): the walk computes, for the cotangent
+    // lam (dL/da per particle, user order), the direct term
+    // gdir_i = -sum_n K_in lam_i and the node sums adj[n] = (sum_i K_in lam_i,
+    // sum_i G g_in (d_in . lam_i)), internal nodes in adj_node, leaves (by
+    // sorted index) in adj_leaf. K = dF/d(com) of the pair force.
+    int adjoint;
+    const float *lamf;  // MIXED
+    const double *lamd; // FP64
+    float *gdirf;       // MIXED: user order, 3 per particle
+    double *gdird;      // FP64
+    double *adj_node;   // 4 doubles per internal node
+    double *adj_leaf;   // 4 doubles per sorted particle
 };
 
 // Launch shape of the persistent walk for this device (blocks to fill every SM).

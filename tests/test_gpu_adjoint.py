@@ -1,0 +1,185 @@
+"""GPU: the adjoint (backward) entry points.
+
+Opening decisions are frozen, so against finite differences of the forward
+pass the agreement holds as long as the perturbation flips no decision (tiny
+steps in the FP64 form); with theta -> 0 the walk opens every node and becomes
+the direct sum, checked against an FP64 direct-sum adjoint written here in numpy."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+G = 6.67384e-11
+
+
+def direct_acc(x, m):
+    d = x[None, :, :] - x[:, None, :]            # d[i, j] = x_j - x_i
+    r2 = (d * d).sum(-1)
+    np.fill_diagonal(r2, np.inf)
+    g = r2 ** -1.5
+    return G * (m[None, :, None] * g[:, :, None] * d).sum(1)
+
+
+def direct_vjp(x, m, la):
+    """(da/dx)^T la and (da/dm)^T la of the direct sum, FP64."""
+    d = x[None, :, :] - x[:, None, :]
+    r2 = (d * d).sum(-1)
+    np.fill_diagonal(r2, np.inf)
+    g = r2 ** -1.5
+    h = -3.0 * r2 ** -2.5
+    s = (d * la[:, None, :]).sum(-1)              # s[i, j] = d_ij . la_i
+    # v[i, j] = G m_j (g la_i + h s d)  : pair Jacobian (w.r.t. x_j) applied to la_i
+    v = G * m[None, :, None] * (g[:, :, None] * la[:, None, :] + (h * s)[:, :, None] * d)
+    gx = -v.sum(1) + v.sum(0)
+    gm = G * (g * s).sum(0)
+    return gx, gm
+
+
+def direct_loss_grad(x0, v0, m, dt, K, target):
+    xs = [x0.copy()]
+    x, v = x0.copy(), v0.copy()
+    for _ in range(K):
+        a = direct_acc(x, m)
+        v = v + a * dt
+        x = x + v * dt
+        xs.append(x.copy())
+    n = len(m)
+    lx = 2.0 * (x - target) / n
+    lv = np.zeros_like(v)
+    lm = np.zeros_like(m)
+    for k in range(K - 1, -1, -1):
+        mu = lv + lx * dt
+        lv = mu
+        gx, gm = direct_vjp(xs[k], m, mu * dt)
+        lx = lx + gx
+        lm = lm + gm
+    return lx, lv, lm
+
+
+def loss(x, target):
+    return ((x - target) ** 2).sum() / len(x)
+
+
+def test_force_vjp_equals_direct_sum_vjp_at_theta_zero(nb):
+    pos, _, mass = nb.generate(300, gen_type=1, seed=5)
+    la = np.random.default_rng(1).standard_normal((300, 3))
+    gx_ref, gm_ref = direct_vjp(pos, mass, la)
+    for prec, tol in ((nb.PRECISION_FP64, 1e-10), (nb.PRECISION_MIXED, 2e-5)):
+        with nb.Engine(precision=prec, theta=1e-9) as e:
+            gx, gm = e.force_vjp(pos, mass, la)
+        assert np.abs(gx - gx_ref).max() <= tol * np.abs(gx_ref).max()
+        assert np.abs(gm - gm_ref).max() <= tol * np.abs(gm_ref).max()
+
+
+@pytest.mark.parametrize("damping", [False, True])
+def test_force_vjp_matches_finite_differences(nb, damping):
+    pos, _, mass = nb.generate(1500, gen_type=1, seed=9)
+    rng = np.random.default_rng(2)
+    la = rng.standard_normal((1500, 3))
+    with nb.Engine(precision=nb.PRECISION_FP64, theta=0.5, damping=int(damping)) as e:
+        gx, gm = e.force_vjp(pos, mass, la)
+        for p in rng.choice(1500, 8, replace=False):
+            for k in range(3):
+                h = 1e-6
+                xp = pos.copy(); xp[p, k] += h
+                xm = pos.copy(); xm[p, k] -= h
+                fd = ((la * e.barnes_hut(xp, mass, damping=damping)).sum()
+                      - (la * e.barnes_hut(xm, mass, damping=damping)).sum()) / (2 * h)
+                assert abs(fd - gx[p, k]) <= 1e-6 * (abs(gx[p, k]) + 1e-3 * np.abs(gx).max()), (p, k, fd, gx[p, k])
+            h = 1e-6 * mass[p]
+            mp = mass.copy(); mp[p] += h
+            mm = mass.copy(); mm[p] -= h
+            fd = ((la * e.barnes_hut(pos, mp, damping=damping)).sum()
+                  - (la * e.barnes_hut(pos, mm, damping=damping)).sum()) / (2 * h)
+            assert abs(fd - gm[p]) <= 1e-6 * (abs(gm[p]) + 1e-3 * np.abs(gm).max()), (p, fd, gm[p])
+
+
+def test_mixed_vjp_close_to_fp64_vjp(nb):
+    pos, _, mass = nb.generate(20000, gen_type=2, size=1024.0)
+    la = np.random.default_rng(3).standard_normal((20000, 3))
+    with nb.Engine(precision=nb.PRECISION_FP64) as e64, nb.Engine() as e32:
+        g64, m64 = e64.force_vjp(pos, mass, la)
+        g32, m32 = e32.force_vjp(pos, mass, la)
+    r = np.linalg.norm(g32 - g64, axis=1) / np.linalg.norm(g64, axis=1)
+    assert np.percentile(r, 99) <= 1e-4
+    assert np.percentile(np.abs(m32 - m64) / np.abs(m64), 99) <= 1e-4
+
+
+def test_backward_equals_direct_sum_reverse_pass(nb):
+    n, K, dt = 200, 6, 0.0333
+    pos, vel, mass = nb.generate(n, gen_type=1, seed=21)
+    target = pos + np.random.default_rng(4).normal(0.0, 5.0, pos.shape)
+    with nb.Engine(precision=nb.PRECISION_FP64, theta=1e-9) as e:
+        e.set_particles(pos, vel, mass)
+        e.forward_checkpointed(K, 4)
+        xK, _ = e.get_particles()
+        gp, gv, gm = e.backward(2.0 * (xK - target) / n)
+    lx, lv, lm = direct_loss_grad(pos, vel, mass, dt, K, target)
+    for a, b in ((gp, lx), (gv, lv), (gm, lm)):
+        assert np.abs(a - b).max() <= 1e-9 * np.abs(b).max()
+
+
+def test_backward_independent_of_checkpoint_interval(nb):
+    n, K = 4096, 8
+    pos, vel, mass = nb.generate(n, gen_type=1, seed=33)
+    target = pos + np.random.default_rng(5).normal(0.0, 5.0, pos.shape)
+    for prec, tol in ((nb.PRECISION_FP64, 1e-11), (nb.PRECISION_MIXED, 1e-5)):
+        with nb.Engine(precision=prec) as e:
+            grads = []
+            for every in (1, 3, 0):
+                e.set_particles(pos, vel, mass)
+                e.forward_checkpointed(K, every)
+                xK, _ = e.get_particles()
+                grads.append(e.backward(2.0 * (xK - target) / n))
+        for g in grads[1:]:
+            for a, b in zip(g, grads[0]):
+                assert np.abs(a - b).max() <= tol * np.abs(b).max()
+
+
+def test_backward_matches_finite_differences(nb):
+    """Central differences of the loss through K steps; theta -> 0 keeps the
+    forward map smooth (no opening decision can flip under the perturbation)."""
+    n, K = 512, 8
+    pos, vel, mass = nb.generate(n, gen_type=1, seed=34)
+    target = pos + np.random.default_rng(7).normal(0.0, 5.0, pos.shape)
+    with nb.Engine(precision=nb.PRECISION_FP64, theta=1e-9) as e:
+        e.set_particles(pos, vel, mass)
+        e.forward_checkpointed(K, 3)
+        xK, _ = e.get_particles()
+        gp, gv, gm = e.backward(2.0 * (xK - target) / n)
+
+        def L(p0, v0, m0):
+            e.set_particles(p0, v0, m0)
+            e.step(K)
+            return loss(e.get_particles()[0], target)
+
+        rng = np.random.default_rng(6)
+        for p in rng.choice(n, 4, replace=False):
+            k = int(rng.integers(3))
+            h = 1e-5
+            xp = pos.copy(); xp[p, k] += h
+            xm = pos.copy(); xm[p, k] -= h
+            fd = (L(xp, vel, mass) - L(xm, vel, mass)) / (2 * h)
+            assert abs(fd - gp[p, k]) <= 1e-6 * np.abs(gp).max() + 1e-4 * abs(gp[p, k]), ("x", p, k, fd, gp[p, k])
+            vp = vel.copy(); vp[p, k] += h
+            vm = vel.copy(); vm[p, k] -= h
+            fd = (L(pos, vp, mass) - L(pos, vm, mass)) / (2 * h)
+            assert abs(fd - gv[p, k]) <= 1e-6 * np.abs(gv).max() + 1e-4 * abs(gv[p, k]), ("v", p, k, fd, gv[p, k])
+            hm = 1e-6 * mass[p]
+            mp = mass.copy(); mp[p] += hm
+            mm = mass.copy(); mm[p] -= hm
+            fd = (L(pos, vel, mp) - L(pos, vel, mm)) / (2 * hm)
+            assert abs(fd - gm[p]) <= 1e-6 * np.abs(gm).max() + 1e-4 * abs(gm[p]), ("m", p, fd, gm[p])
+
+
+def test_backward_state_errors(nb):
+    with nb.Engine(adaptive=1) as e:
+        pos, vel, mass = nb.generate(100)
+        e.set_particles(pos, vel, mass)
+        with pytest.raises(nb.NBodyError) as ex:
+            e.forward_checkpointed(4)
+        assert ex.value.status == nb.ERR_INVALID
+    with nb.Engine() as e:
+        e.set_particles(pos, vel, mass)
+        with pytest.raises(nb.NBodyError) as ex:
+            e.backward(np.zeros((100, 3)))
+        assert ex.value.status == nb.ERR_STATE
