@@ -42,13 +42,16 @@ WORKLOAD = dict(gen_type=2, n=1 << 20, r_sphere=100.0, rotation_magnitude=0.1, s
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=WORKLOAD["n"])
     ap.add_argument("--theta", type=float, default=0.5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU walk seconds of the sample")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-fd", type=int, default=0,
+                    help="also check the config-4 gradient against central differences on this many coordinates")
     return ap.parse_args()
 
 
@@ -81,7 +84,7 @@ class Clocks:
     def __enter__(self):
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.p = None
@@ -298,6 +301,26 @@ def run_ours(args) -> None:
             pg.destroy_process_group()
         return
 
+    # ---- the plain FP64 form on the same workload, same initial state, same K
+    fp64_ms_step = None
+    with nb.Engine(nb.default_params(theta=args.theta, adaptive=1, min_adaptive_dt=0.00333, max_pos_change=3.0,
+                                     max_vel_change=3.0, precision=nb.PRECISION_FP64, device=local)) as e64:
+        e64._lib.nbody_set_stream(e64._h, C_void(stream.cuda_stream))
+        e64.set_particles(pos0, vel0, mass)
+        e64.step(args.warmup)
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        e64.step(args.steps)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        fp64_ms_step = f0.elapsed_time(f1) / args.steps
+
+    # ---- adjoint / forward at the adjoint configuration (sphere N=65536, K=256, checkpoint 16)
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_leg(nb, torch, stream, local, args.adjoint_fd)
+
     # ---- accuracy on the initial state: vs the FP64 form (same lists) and FP64 direct sum
     acc_mixed, counts = eng.barnes_hut(pos0, mass, theta=args.theta, counts=True)
     with nb.Engine(nb.default_params(theta=args.theta, precision=nb.PRECISION_FP64, device=local)) as e64:
@@ -351,9 +374,12 @@ def run_ours(args) -> None:
         "phases_ms": {k: float(np.mean(v)) for k, v in ph.items() if k != "inter"},
         "walk_interactions_per_s": walk_inter / (walk_ms * 1e-3),
         "fp64_form_walk_ms": fp64_walk_ms,
+        "fp64_form_ms_per_step": fp64_ms_step,
+        "speedup_vs_fp64_form": fp64_ms_step / ms_step if fp64_ms_step else None,
         "p99_rel_err_vs_fp64_form": p99_vs_fp64,
         "vs_fp64_direct_sum": direct,
-        "adjoint_fwd_ratio": None,
+        "adjoint_fwd_ratio": adjoint["ratio"] if adjoint else None,
+        "adjoint": adjoint,
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 56 * args.n,
                 "d2h_bytes_per_step": 48 * args.n},
@@ -370,6 +396,58 @@ def run_ours(args) -> None:
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def adjoint_leg(nb, torch, stream, device, fd_coords=0):
+    """Config 4: sphere N=65536, theta 0.5, fixed dt 0.0333, K=256 steps,
+    checkpoint every 16; loss = mean squared distance of the final positions to
+    a seeded Gaussian-perturbed (sigma 5) copy of the initial positions."""
+    n, K, every = 65536, 256, 16
+    pos, vel, mass = nb.generate(n, gen_type=1, r_sphere=100.0, rotation_magnitude=0.1, seed=0xDEADBEEF)
+    target = pos + np.random.default_rng(0xDEADBEEF).normal(0.0, 5.0, pos.shape)
+    out = {"config": "sphere N=65536 theta=0.5 dt=0.0333 K=256 checkpoint 16", "precision": "mixed"}
+    with nb.Engine(nb.default_params(theta=0.5, dt=0.0333, device=device)) as e:
+        e._lib.nbody_set_stream(e._h, C_void(stream.cuda_stream))
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+        e.set_particles(pos, vel, mass)
+        e.step(4)  # warm-up (allocations, code)
+        e.set_particles(pos, vel, mass)
+        ev[0].record(stream)
+        e.step(K)
+        ev[1].record(stream)
+        e.set_particles(pos, vel, mass)
+        ev[2].record(stream)
+        e.forward_checkpointed(K, every)
+        ev[3].record(stream)
+        xK, _ = e.get_particles()
+        gsrc = 2.0 * (xK - target) / n
+        ev[4].record(stream)
+        gp, gv, gm = e.backward(gsrc)
+        ev[5].record(stream)
+        torch.cuda.synchronize()
+        fwd = ev[0].elapsed_time(ev[1])
+        fwd_ck = ev[2].elapsed_time(ev[3])
+        bwd = ev[4].elapsed_time(ev[5])
+        out.update(forward_ms=fwd, forward_checkpointed_ms=fwd_ck, backward_ms=bwd, ratio=bwd / fwd,
+                   loss=float(((xK - target) ** 2).sum() / n))
+        if fd_coords:
+            rng = np.random.default_rng(0xDEADBEEF)
+            idx = rng.choice(3 * n, fd_coords, replace=False)
+            rel = []
+            for q in idx:
+                p, k = divmod(int(q), 3)
+                h = 1e-3 * max(abs(pos[p, k]), 1e-3)
+                vals = []
+                for sgn in (1, -1):
+                    x0 = pos.copy(); x0[p, k] += sgn * h
+                    e.set_particles(x0, vel, mass)
+                    e.step(K)
+                    vals.append(float(((e.get_particles()[0] - target) ** 2).sum() / n))
+                fd = (vals[0] - vals[1]) / (2 * h)
+                rel.append(abs(fd - gp[p, k]) / max(abs(fd), abs(gp[p, k]), 1e-300))
+            out["fd_check"] = {"coords": fd_coords, "eps": "1e-3 relative", "median_rel": float(np.median(rel)),
+                               "max_rel": float(np.max(rel)), "frac_le_1e-4": float(np.mean(np.array(rel) <= 1e-4))}
+    return out
 
 
 def C_void(x):
