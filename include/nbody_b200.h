@@ -95,6 +95,13 @@ int nbody_barnes_hut(nbody_ctx *ctx, uint32_t n, const double *pos, const double
  * the particle state kept in device memory between steps. */
 int nbody_set_particles(nbody_ctx *ctx, uint32_t n, const double *pos, const double *vel,
                         const double *mass);
+/* Declares the resident particles to be `nsys` independent systems stored one
+ * after another, counts[s] particles each (every count >= 1). Each system gets
+ * its own root cube and octree (as if it were its own reference run); one
+ * persistent walk serves all systems from a shared work queue of 32-particle
+ * groups. nsys = 1 restores a single system. nbody_barnes_hut always treats its
+ * input as one system. (No reference counterpart: the reference runs one system.) */
+int nbody_set_systems(nbody_ctx *ctx, uint32_t nsys, const uint32_t *counts);
 /* Any output pointer may be NULL. acc is the last computed acceleration. */
 int nbody_get_particles(nbody_ctx *ctx, double *pos, double *vel, double *acc);
 /* nsteps full steps: root cube -> octree -> mass/COM -> walk+force -> (adaptive dt) -> update. */
@@ -136,8 +143,13 @@ typedef struct nbody_stats {
     float ms_tree, ms_com, ms_walk, ms_update; /* last pass, CUDA events; 0 if not timed */
 } nbody_stats;
 int nbody_get_stats(nbody_ctx *ctx, nbody_stats *out);
-/* Time phases with CUDA events on the context stream (default off). */
+/* Time phases with CUDA events on the context stream (default off; timed calls
+ * launch kernels one by one). */
 int nbody_set_timing(nbody_ctx *ctx, int enabled);
+/* Replay captured CUDA graphs for steps and adjoint steps (default on). Each
+ * distinct configuration is captured on first use; a stream that cannot be
+ * captured (the legacy default stream) falls back to direct launches. */
+int nbody_set_graphs(nbody_ctx *ctx, int enabled);
 
 typedef struct nbody_diagnostics {
     double kinetic;          /* sum 1/2 m v^2 */

@@ -105,6 +105,7 @@ _SIGS = {
     "nbody_barnes_hut": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int, C.c_double,
                                    C.c_void_p, C.c_void_p]),
     "nbody_set_particles": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "nbody_set_systems": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p]),
     "nbody_get_particles": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "nbody_step": (C.c_int, [C.c_void_p, C.c_uint32]),
     "nbody_compute_forces": (C.c_int, [C.c_void_p]),
@@ -112,6 +113,7 @@ _SIGS = {
     "nbody_device_view_get": (C.c_int, [C.c_void_p, C.POINTER(DeviceView)]),
     "nbody_get_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "nbody_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "nbody_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
     "nbody_get_diagnostics": (C.c_int, [C.c_void_p, C.POINTER(Diagnostics)]),
     "nbody_default_gen_params": (None, [C.POINTER(GenParams)]),
     "nbody_generate": (C.c_int, [C.POINTER(GenParams), C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -249,6 +251,9 @@ class Engine:
             setattr(self.params, k, v)
         _check(self._lib.nbody_set_params(self._h, C.byref(self.params)))
 
+    def set_graphs(self, on: bool = True) -> None:
+        _check(self._lib.nbody_set_graphs(self._h, int(on)))
+
     def set_timing(self, on: bool = True) -> None:
         _check(self._lib.nbody_set_timing(self._h, int(on)))
 
@@ -262,6 +267,11 @@ class Engine:
         _check(self._lib.nbody_barnes_hut(self._h, n, pos.ctypes.data, mass.ctypes.data, int(damping),
                                           float(theta), acc.ctypes.data, _ptr(cnt)))
         return (acc, cnt) if counts else acc
+
+    def set_systems(self, counts) -> None:
+        """Independent systems stored one after another (counts per system)."""
+        counts = np.ascontiguousarray(counts, dtype=np.uint32)
+        _check(self._lib.nbody_set_systems(self._h, len(counts), counts.ctypes.data))
 
     def set_particles(self, pos, vel, mass) -> None:
         pos = _aos(pos)

@@ -13,7 +13,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <new>
+#include <vector>
 
 #include "../../include/nbody_b200.h"
 #include "step.cuh"
@@ -80,6 +82,23 @@ struct nbody_ctx {
     uint32_t fwd_steps = 0, fwd_every = 0, fwd_n = 0;
     double fwd_dt = 0.0;
     bool have_fwd = false;
+    // independent systems (nbody_set_systems)
+    uint32_t nsys = 1, sys_total = 0, ngroups = 0;
+    void *sys_arena = nullptr;
+    size_t sys_bytes = 0;
+    uint32_t *sys_start = nullptr, *sys_id = nullptr, *sys_sorted = nullptr;
+    int4 *groups = nullptr;
+    double *sys_root = nullptr;
+    int32_t *sys_root_node = nullptr;
+    bool single_pass = false;  // nbody_barnes_hut: one system regardless of the layout
+    // CUDA graphs: one captured step replayed per step; per-offset graphs for the
+    // adjoint's recompute and reverse steps. Rebuilt when their key changes.
+    bool use_graphs = true;
+    std::vector<unsigned char> step_key, adj_key;
+    cudaGraphExec_t step_exec = nullptr;
+    unsigned step_launches = 0;
+    std::vector<cudaGraphExec_t> rec_exec, adj_exec;
+    std::vector<unsigned> rec_launches, adj_launches;
 };
 
 namespace {
@@ -210,6 +229,13 @@ int force_pass(nbody_ctx *c, int damping, double theta, bool fp64, bool want_vma
     NB_CUDA(launch_reset_pass(c->sc, c->stream));
     tree_inputs(c, n, want_vmax);
     if (pos) c->tb.pos = pos;
+    const bool multi = c->nsys > 1 && !c->single_pass && c->sys_total == n;
+    c->tb.nsys = multi ? c->nsys : 1;
+    c->tb.sys_start = c->sys_start;
+    c->tb.sys_id = c->sys_id;
+    c->tb.sys_sorted = c->sys_sorted;
+    c->tb.sys_root = c->sys_root;
+    c->tb.sys_root_node = c->sys_root_node;
     ev(c, 0);
     NB_CUDA(build_octree(c->tb, c->stream, &launches));
     ev(c, 1);
@@ -231,7 +257,10 @@ int force_pass(nbody_ctx *c, int damping, double theta, bool fp64, bool want_vma
     a.pot = want_pot ? c->pot : nullptr;
     a.spill = c->spill;
     a.spill_cap = kSpillCap;
-    a.n_groups = (n + 31) / 32;
+    a.n_groups = multi ? c->ngroups : (n + 31) / 32;
+    a.groups = multi ? c->groups : nullptr;
+    a.sys_root_node = c->sys_root_node;
+    a.sys_root = c->sys_root;
     a.track_max_acc = track_amax ? 1 : 0;
     if (adjoint) {
         a.adjoint = 1;
@@ -292,14 +321,92 @@ int download_acc(nbody_ctx *c, double *acc) {
     return NBODY_OK;
 }
 
-int run_steps(nbody_ctx *c, uint32_t nsteps) {
+// ---- CUDA graphs ---------------------------------------------------------------
+// Everything a captured sequence depends on; a change forces a new capture.
+std::vector<unsigned char> graph_key(nbody_ctx *c, uint32_t extra) {
+    struct K {
+        uint32_t n, nsys, ngroups, extra;
+        void *arena, *adj, *sys, *stream;
+        nbody_params p;
+        WalkLaunch wm, wf;
+    } k;
+    std::memset(&k, 0, sizeof k);
+    k.n = c->n; k.nsys = c->nsys; k.ngroups = c->ngroups; k.extra = extra;
+    k.arena = c->arena; k.adj = c->adj_arena; k.sys = c->sys_arena; k.stream = (void *)c->stream;
+    k.p = c->p; k.wm = c->wl_mixed; k.wf = c->wl_fp64;
+    const unsigned char *b = (const unsigned char *)&k;
+    return std::vector<unsigned char>(b, b + sizeof k);
+}
+
+void drop_graph(cudaGraphExec_t &g) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+}
+
+void drop_graphs(nbody_ctx *c) {
+    drop_graph(c->step_exec);
+    for (auto &g : c->rec_exec) drop_graph(g);
+    for (auto &g : c->adj_exec) drop_graph(g);
+    c->rec_exec.clear(); c->adj_exec.clear();
+    c->rec_launches.clear(); c->adj_launches.clear();
+    c->step_key.clear(); c->adj_key.clear();
+}
+
+// Captures what `body` enqueues on the context stream into an executable graph.
+// Returns false (nothing captured, no error left behind) when capture is not
+// possible on this stream; the caller then launches directly.
+template <class F>
+bool capture(nbody_ctx *c, cudaGraphExec_t *out, unsigned *launches, F &&body) {
+    *out = nullptr;
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    const unsigned long long l0 = c->launches;
+    const int rc = body();
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    bool ok = rc == NBODY_OK && e == cudaSuccess && g;
+    if (ok) ok = cudaGraphInstantiate(out, g, 0) == cudaSuccess;
+    if (g) cudaGraphDestroy(g);
+    *launches = (unsigned)(c->launches - l0);
+    c->launches = l0;
+    if (!ok) {
+        cudaGetLastError();
+        *out = nullptr;
+    }
+    return ok;
+}
+
+int one_step(nbody_ctx *c) {
     const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
     StepParams sp{c->p.dt, c->p.adaptive, c->p.min_adaptive_dt, c->p.max_pos_change, c->p.max_vel_change};
+    int rc = force_pass(c, c->p.damping, c->p.theta, fp64, c->p.adaptive != 0, c->p.adaptive != 0, false, false);
+    if (rc) return rc;
+    NB_CUDA(launch_update(c->pos, c->vel, c->acc, fp64, c->n, sp, c->sc, c->stream));
+    c->launches++;
+    return NBODY_OK;
+}
+
+int run_steps(nbody_ctx *c, uint32_t nsteps) {
+    if (c->use_graphs && !c->timing) {
+        auto key = graph_key(c, 0);
+        if (!c->step_exec || key != c->step_key) {
+            drop_graph(c->step_exec);
+            c->step_key.clear();
+            if (capture(c, &c->step_exec, &c->step_launches, [&] { return one_step(c); })) c->step_key = key;
+        }
+        if (c->step_exec) {
+            for (uint32_t s = 0; s < nsteps; s++) {
+                NB_CUDA(cudaGraphLaunch(c->step_exec, c->stream));
+                c->launches += c->step_launches;
+            }
+            return NBODY_OK;
+        }
+    }
     for (uint32_t s = 0; s < nsteps; s++) {
-        int rc = force_pass(c, c->p.damping, c->p.theta, fp64, c->p.adaptive != 0, c->p.adaptive != 0, false, false);
+        int rc = one_step(c);
         if (rc) return rc;
-        NB_CUDA(launch_update(c->pos, c->vel, c->acc, fp64, c->n, sp, c->sc, c->stream));
-        c->launches++;
         ev(c, 4);
     }
     return NBODY_OK;
@@ -358,6 +465,25 @@ int step_on(nbody_ctx *c, double *pos, double *vel, bool fp64) {
     NB_CUDA(launch_update(pos, vel, c->acc, fp64, c->n, sp, c->sc, c->stream));
     c->launches++;
     return NBODY_OK;
+}
+
+// Runs `body` through the graph cached at slot i (capturing it on first use).
+template <class F>
+int run_cached(nbody_ctx *c, std::vector<cudaGraphExec_t> &execs, std::vector<unsigned> &launches, uint32_t i,
+               F &&body) {
+    if (c->use_graphs && !c->timing) {
+        if (execs.size() <= i) {
+            execs.resize(i + 1, nullptr);
+            launches.resize(i + 1, 0);
+        }
+        if (!execs[i]) capture(c, &execs[i], &launches[i], body);
+        if (execs[i]) {
+            NB_CUDA(cudaGraphLaunch(execs[i], c->stream));
+            c->launches += launches[i];
+            return NBODY_OK;
+        }
+    }
+    return body();
 }
 
 #define CTX_OR_FAIL(c)                                                 \
@@ -425,8 +551,10 @@ int nbody_destroy(nbody_ctx *c) {
     if (!c) return NBODY_OK;
     cudaSetDevice(c->p.device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graphs(c);
     if (c->arena) cudaFree(c->arena);
     if (c->adj_arena) cudaFree(c->adj_arena);
+    if (c->sys_arena) cudaFree(c->sys_arena);
     if (c->sc) cudaFree(c->sc);
     if (c->hsc) cudaFreeHost(c->hsc);
     for (auto &e : c->ev)
@@ -449,9 +577,18 @@ int nbody_set_params(nbody_ctx *c, const nbody_params *p) {
 int nbody_set_stream(nbody_ctx *c, void *stream) {
     CTX_OR_FAIL(c);
     NB_CUDA(cudaStreamSynchronize(c->stream));
+    drop_graphs(c);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     c->stream = (cudaStream_t)stream;
     c->own_stream = false;
+    return NBODY_OK;
+}
+
+int nbody_set_graphs(nbody_ctx *c, int enabled) {
+    CTX_OR_FAIL(c);
+    NB_CUDA(cudaStreamSynchronize(c->stream));
+    drop_graphs(c);
+    c->use_graphs = enabled != 0;
     return NBODY_OK;
 }
 
@@ -472,7 +609,9 @@ int nbody_barnes_hut(nbody_ctx *c, uint32_t n, const double *pos, const double *
     if (rc) return rc;
     if ((rc = begin_call(c))) return rc;
     const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
+    c->single_pass = true;
     rc = force_pass(c, damping ? 1 : 0, theta, fp64, false, false, counts_out != nullptr, false);
+    c->single_pass = false;
     if (rc) return rc;
     ev(c, 4);
     if ((rc = download_acc(c, acc_out))) return rc;
@@ -481,9 +620,71 @@ int nbody_barnes_hut(nbody_ctx *c, uint32_t n, const double *pos, const double *
     return check_status(c);
 }
 
+int nbody_set_systems(nbody_ctx *c, uint32_t nsys, const uint32_t *counts) {
+    CTX_OR_FAIL(c);
+    if (nsys == 0 || nsys > 65536 || (nsys > 1 && !counts)) return fail(NBODY_ERR_INVALID, "1 <= nsys <= 65536%s");
+    if (nsys == 1) {
+        c->nsys = 1;
+        c->sys_total = 0;
+        return NBODY_OK;
+    }
+    uint64_t total = 0;
+    uint32_t ngroups = 0;
+    for (uint32_t k = 0; k < nsys; k++) {
+        if (counts[k] == 0) return fail(NBODY_ERR_INVALID, "every system needs at least one particle%s");
+        total += counts[k];
+        ngroups += (counts[k] + 31) / 32;
+    }
+    if (total > kMaxParticles) return fail(NBODY_ERR_INVALID, "total exceeds the 2^28 particle limit%s");
+    const size_t N = total;
+    struct Piece { void **dst; size_t bytes; };
+    Piece pieces[] = {{(void **)&c->sys_start, 4 * ((size_t)nsys + 1)}, {(void **)&c->sys_id, 4 * N},
+                      {(void **)&c->sys_sorted, 4 * N}, {(void **)&c->groups, 16 * (size_t)ngroups},
+                      {(void **)&c->sys_root, 32 * (size_t)nsys}, {(void **)&c->sys_root_node, 4 * (size_t)nsys}};
+    size_t bytes = 0;
+    for (auto &pc : pieces) bytes += align256(pc.bytes);
+    if (bytes > c->sys_bytes) {
+        NB_CUDA(cudaStreamSynchronize(c->stream));
+        if (c->sys_arena) NB_CUDA(cudaFree(c->sys_arena));
+        c->sys_arena = nullptr;
+        c->sys_bytes = 0;
+        cudaError_t e = cudaMalloc(&c->sys_arena, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(NBODY_ERR_OOM, "system tables (%s)", cudaGetErrorString(e));
+        }
+        c->sys_bytes = bytes;
+    }
+    char *p = (char *)c->sys_arena;
+    for (auto &pc : pieces) {
+        *pc.dst = p;
+        p += align256(pc.bytes);
+    }
+    std::vector<uint32_t> start(nsys + 1), sid(N);
+    std::vector<int4> groups;
+    groups.reserve(ngroups);
+    start[0] = 0;
+    for (uint32_t k = 0; k < nsys; k++) {
+        start[k + 1] = start[k] + counts[k];
+        for (uint32_t i = start[k]; i < start[k + 1]; i++) sid[i] = k;
+        for (uint32_t o = 0; o < counts[k]; o += 32)
+            groups.push_back(make_int4((int)(start[k] + o), (int)std::min(32u, counts[k] - o), (int)k, 0));
+    }
+    NB_CUDA(cudaMemcpyAsync(c->sys_start, start.data(), 4 * start.size(), cudaMemcpyHostToDevice, c->stream));
+    NB_CUDA(cudaMemcpyAsync(c->sys_id, sid.data(), 4 * N, cudaMemcpyHostToDevice, c->stream));
+    NB_CUDA(cudaMemcpyAsync(c->groups, groups.data(), 16 * groups.size(), cudaMemcpyHostToDevice, c->stream));
+    NB_CUDA(cudaStreamSynchronize(c->stream));
+    c->nsys = nsys;
+    c->sys_total = (uint32_t)total;
+    c->ngroups = ngroups;
+    return NBODY_OK;
+}
+
 int nbody_set_particles(nbody_ctx *c, uint32_t n, const double *pos, const double *vel, const double *mass) {
     CTX_OR_FAIL(c);
     if (n > kMaxParticles) return fail(NBODY_ERR_INVALID, "n exceeds the 2^28 particle limit%s");
+    if (c->nsys > 1 && n != c->sys_total)
+        return fail(NBODY_ERR_INVALID, "n differs from the total of the systems declared by nbody_set_systems%s");
     if (n && (!pos || !mass)) return fail(NBODY_ERR_INVALID, "null array%s");
     int rc = upload(c, n, pos, vel, mass);
     if (rc) return rc;
@@ -638,13 +839,13 @@ int nbody_forward_checkpointed(nbody_ctx *c, uint32_t nsteps, uint32_t every) {
     if ((rc = begin_call(c))) return rc;
     const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
     const size_t N3 = 3 * (size_t)c->n;
-    for (uint32_t k = 0; k < nsteps; k++) {
-        if (k % every == 0) {
-            double *ck = c->ckpt + 2 * N3 * (k / every);
-            NB_CUDA(cudaMemcpyAsync(ck, c->pos, 8 * N3, cudaMemcpyDeviceToDevice, c->stream));
-            NB_CUDA(cudaMemcpyAsync(ck + N3, c->vel, 8 * N3, cudaMemcpyDeviceToDevice, c->stream));
-        }
-        if ((rc = step_on(c, c->pos, c->vel, fp64))) return rc;
+    (void)fp64;
+    for (uint32_t k = 0; k < nsteps; k += every) {
+        double *ck = c->ckpt + 2 * N3 * (k / every);
+        NB_CUDA(cudaMemcpyAsync(ck, c->pos, 8 * N3, cudaMemcpyDeviceToDevice, c->stream));
+        NB_CUDA(cudaMemcpyAsync(ck + N3, c->vel, 8 * N3, cudaMemcpyDeviceToDevice, c->stream));
+        const uint32_t len = nsteps - k < every ? nsteps - k : every;
+        if ((rc = run_steps(c, len))) return rc;
     }
     if ((rc = copy_scalars_back(c))) return rc;
     if ((rc = check_status(c))) return rc;
@@ -667,6 +868,16 @@ int nbody_backward(nbody_ctx *c, const double *dL_dpos, const double *dL_dvel, d
     if (c->p.dt != c->fwd_dt) return fail(NBODY_ERR_STATE, "dt changed since the forward pass%s");
     int rc = begin_call(c);
     if (rc) return rc;
+    {
+        auto key = graph_key(c, C);
+        if (key != c->adj_key) {
+            for (auto &g : c->rec_exec) drop_graph(g);
+            for (auto &g : c->adj_exec) drop_graph(g);
+            c->rec_exec.clear(); c->adj_exec.clear();
+            c->rec_launches.clear(); c->adj_launches.clear();
+            c->adj_key = key;
+        }
+    }
     NB_CUDA(cudaMemcpyAsync(c->lx, dL_dpos, 8 * N3, cudaMemcpyHostToDevice, c->stream));
     if (dL_dvel) NB_CUDA(cudaMemcpyAsync(c->lv, dL_dvel, 8 * N3, cudaMemcpyHostToDevice, c->stream));
     else NB_CUDA(cudaMemsetAsync(c->lv, 0, 8 * N3, c->stream));
@@ -678,19 +889,26 @@ int nbody_backward(nbody_ctx *c, const double *dL_dpos, const double *dL_dvel, d
         NB_CUDA(cudaMemcpyAsync(c->seg_pos, ck, 8 * N3, cudaMemcpyDeviceToDevice, c->stream));
         NB_CUDA(cudaMemcpyAsync(c->vel_work, ck + N3, 8 * N3, cudaMemcpyDeviceToDevice, c->stream));
         for (uint32_t i = 0; i + 1 < len; i++) {
-            double *xi = c->seg_pos + N3 * i, *xn = xi + N3;
-            NB_CUDA(cudaMemcpyAsync(xn, xi, 8 * N3, cudaMemcpyDeviceToDevice, c->stream));
-            // forces at xi, then update the copy in place: x_{k+1}, v_{k+1}
-            rc = force_pass(c, c->p.damping, c->p.theta, fp64, false, false, false, false, xi, false);
-            if (rc) return rc;
-            StepParams sp{c->p.dt, 0, 0, 0, 0};
-            NB_CUDA(launch_update(xn, c->vel_work, c->acc, fp64, n, sp, c->sc, c->stream));
-            c->launches++;
+            auto rec = [&, i]() -> int {
+                double *xi = c->seg_pos + N3 * i, *xn = xi + N3;
+                NB_CUDA(cudaMemcpyAsync(xn, xi, 8 * N3, cudaMemcpyDeviceToDevice, c->stream));
+                // forces at xi, then update the copy in place: x_{k+1}, v_{k+1}
+                int r = force_pass(c, c->p.damping, c->p.theta, fp64, false, false, false, false, xi, false);
+                if (r) return r;
+                StepParams sp{c->p.dt, 0, 0, 0, 0};
+                NB_CUDA(launch_update(xn, c->vel_work, c->acc, fp64, n, sp, c->sc, c->stream));
+                c->launches++;
+                return NBODY_OK;
+            };
+            if ((rc = run_cached(c, c->rec_exec, c->rec_launches, i, rec))) return rc;
         }
         for (int i = (int)len - 1; i >= 0; i--) {
-            NB_CUDA(launch_adj_pre(c->lx, c->lv, c->lam, fp64, c->p.dt, n, c->stream));
-            c->launches++;
-            if ((rc = adjoint_force(c, c->seg_pos + N3 * (size_t)i, c->p.damping, c->p.theta, fp64))) return rc;
+            auto adj = [&, i]() -> int {
+                NB_CUDA(launch_adj_pre(c->lx, c->lv, c->lam, fp64, c->p.dt, n, c->stream));
+                c->launches++;
+                return adjoint_force(c, c->seg_pos + N3 * (size_t)i, c->p.damping, c->p.theta, fp64);
+            };
+            if ((rc = run_cached(c, c->adj_exec, c->adj_launches, (uint32_t)i, adj))) return rc;
         }
     }
     NB_CUDA(cudaMemcpyAsync(dL_dpos0, c->lx, 8 * N3, cudaMemcpyDeviceToHost, c->stream));

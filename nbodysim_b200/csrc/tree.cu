@@ -85,6 +85,45 @@ __global__ void k_bbox(const double *__restrict__ pos, const double *__restrict_
     }
 }
 
+// Root cube per system (several independent systems): one block per system.
+__global__ void k_bbox_systems(const double *__restrict__ pos, const double *__restrict__ mass,
+                               const uint32_t *__restrict__ sys_start, double *__restrict__ sys_root,
+                               DevScalars *sc) {
+    __shared__ double s_red[6][32];
+    const uint32_t b0 = sys_start[blockIdx.x], b1 = sys_start[blockIdx.x + 1];
+    double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    bool bad = false;
+    for (uint32_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+        const double x = pos[3 * (size_t)i], y = pos[3 * (size_t)i + 1], z = pos[3 * (size_t)i + 2];
+        bad |= !(isfinite(x) && isfinite(y) && isfinite(z) && isfinite(mass[i]));
+        mn[0] = fmin(mn[0], x); mx[0] = fmax(mx[0], x);
+        mn[1] = fmin(mn[1], y); mx[1] = fmax(mx[1], y);
+        mn[2] = fmin(mn[2], z); mx[2] = fmax(mx[2], z);
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&sc->status, kStatusNonFinite);
+    double v[6] = {mn[0], mn[1], mn[2], -mx[0], -mx[1], -mx[2]};
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int k = 0; k < 6; k++) {
+        const double r = warp_min(v[k]);
+        if (lane == 0) s_red[k][wid] = r;
+    }
+    __syncthreads();
+    if (wid != 0) return;
+    double r[6];
+    for (int k = 0; k < 6; k++) r[k] = warp_min(lane < nw ? s_red[k][lane] : INFINITY);
+    if (lane == 0) {
+        const double lo[3] = {r[0], r[1], r[2]}, hi[3] = {-r[3], -r[4], -r[5]};
+        double *o = sys_root + 4 * (size_t)blockIdx.x;
+        for (int k = 0; k < 3; k++) o[k] = (lo[k] + hi[k]) / 2.0;
+        const double ex = hi[0] - lo[0], ey = hi[1] - lo[1], ez = hi[2] - lo[2];
+        double side;
+        if (ex > ey && ex > ez) side = ex + 2.0;
+        else if (ey > ex && ey > ez) side = ey + 2.0;
+        else side = ez + 2.0;
+        o[3] = side;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Octant digits by descent from the root cube, rounding every child centre
 // exactly as allocate_child does (src/octree.cpp:65-84: center + (+-1 * half) / 2
@@ -113,11 +152,18 @@ __device__ inline uint64_t descend_word(double x, double y, double z, double &cx
 // bulk of the system, so the first 21 levels alone do not separate it.
 __global__ void k_keys(const double *__restrict__ pos, uint32_t n, const DevScalars *sc,
                        uint64_t *__restrict__ k1_user, uint64_t *__restrict__ k2_sortkey,
-                       uint64_t *__restrict__ k2_user, uint32_t *__restrict__ idx) {
+                       uint64_t *__restrict__ k2_user, uint32_t *__restrict__ idx,
+                       const uint32_t *__restrict__ sys_id, const double *__restrict__ sys_root) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    double cx = sc->root_center[0], cy = sc->root_center[1], cz = sc->root_center[2];
-    double side = sc->root_side;
+    double cx, cy, cz, side;
+    if (sys_id) {
+        const double *r = sys_root + 4 * (size_t)sys_id[i];
+        cx = r[0]; cy = r[1]; cz = r[2]; side = r[3];
+    } else {
+        cx = sc->root_center[0]; cy = sc->root_center[1]; cz = sc->root_center[2];
+        side = sc->root_side;
+    }
     const double x = pos[3 * (size_t)i], y = pos[3 * (size_t)i + 1], z = pos[3 * (size_t)i + 2];
     const uint64_t a = descend_word(x, y, z, cx, cy, cz, side);
     const uint64_t b = descend_word(x, y, z, cx, cy, cz, side);
@@ -131,6 +177,15 @@ __global__ void k_gather_key(const uint64_t *__restrict__ src, const uint32_t *_
                              uint64_t *__restrict__ dst, uint32_t n) {
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j < n) dst[j] = src[idx[j]];
+}
+
+__global__ void k_gather_sys(const uint32_t *__restrict__ sys_id, const uint32_t *__restrict__ idx,
+                             uint64_t *__restrict__ key, uint32_t *__restrict__ sys_sorted, uint32_t n) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint32_t s = sys_id[idx[j]];
+    if (key) key[j] = s;
+    if (sys_sorted) sys_sorted[j] = s;
 }
 
 // ---------------------------------------------------------------------------
@@ -291,14 +346,17 @@ constexpr int kMaxDeepGroup = 64;
 
 __global__ void k_deep_groups(const uint64_t *__restrict__ key1, const uint64_t *__restrict__ key2,
                               uint64_t *__restrict__ key3, uint32_t *__restrict__ idx,
-                              double4 *__restrict__ body, uint32_t n, DevScalars *sc) {
+                              double4 *__restrict__ body, uint32_t n, const uint32_t *__restrict__ sys,
+                              const double *__restrict__ sys_root, DevScalars *sc) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i + 1 >= n) return;
     const uint64_t k = key1[i], kk = key2[i];
-    if (key1[i + 1] != k || key2[i + 1] != kk) return;
-    if (i > 0 && key1[i - 1] == k && key2[i - 1] == kk) return;  // not the first of its group
+    const uint32_t ss = sys ? sys[i] : 0u;
+    auto same = [&](uint32_t q) { return key1[q] == k && key2[q] == kk && (!sys || sys[q] == ss); };
+    if (!same(i + 1)) return;
+    if (i > 0 && same(i - 1)) return;  // not the first of its group
     uint32_t e = i + 1;
-    while (e + 1 < n && key1[e + 1] == k && key2[e + 1] == kk) e++;
+    while (e + 1 < n && same(e + 1)) e++;
     const uint32_t g = e - i + 1;
     atomicAdd(&sc->deep_groups, 1u);
     atomicOr(&sc->status, kStatusDeepGroup);
@@ -310,8 +368,12 @@ __global__ void k_deep_groups(const uint64_t *__restrict__ key1, const uint64_t 
         atomicOr(&sc->status, kStatusCoincident);
         return;
     }
-    const double rcx = sc->root_center[0], rcy = sc->root_center[1], rcz = sc->root_center[2];
-    const double rs = sc->root_side;
+    double rcx = sc->root_center[0], rcy = sc->root_center[1], rcz = sc->root_center[2];
+    double rs = sc->root_side;
+    if (sys) {
+        const double *r = sys_root + 4 * (size_t)ss;
+        rcx = r[0]; rcy = r[1]; rcz = r[2]; rs = r[3];
+    }
     for (uint32_t j = i; j <= e; j++) {
         const double4 b = body[j];
         double cx = rcx, cy = rcy, cz = rcz, s = rs;
@@ -343,8 +405,10 @@ __global__ void k_deep_groups(const uint64_t *__restrict__ key1, const uint64_t 
 struct KeyView {
     const uint64_t *k1, *k2, *k3;
     int n;
+    const uint32_t *sys;  // system per sorted position, or null (one system)
     __device__ int delta(int i, int j) const {
         if (j < 0 || j >= n) return -1;
+        if (sys && sys[i] != sys[j]) return -1;  // separate systems: separate trees
         uint64_t a = k1[i], b = k1[j];
         if (a != b) return __clzll(a ^ b) - 1;
         a = k2[i]; b = k2[j];
@@ -363,6 +427,13 @@ __global__ void k_radix_tree(KeyView kv, int32_t *__restrict__ bleft, int32_t *_
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = kv.n;
     if (i >= n - 1) return;
+    // With several systems, the internal nodes of the system [s, e) are s..e-2:
+    // the last particle of a system indexes no internal node.
+    if (kv.sys && kv.sys[i] != kv.sys[i + 1]) {
+        bdelta[i] = -1;
+        return;
+    }
+    const bool seg_root = i == 0 || (kv.sys && kv.sys[i - 1] != kv.sys[i]);
     int d = (kv.delta(i, i + 1) - kv.delta(i, i - 1)) >= 0 ? 1 : -1;
     int dmin = kv.delta(i, i - d);
     int lmax = 2;
@@ -387,7 +458,7 @@ __global__ void k_radix_tree(KeyView kv, int32_t *__restrict__ bleft, int32_t *_
     bdelta[i] = dnode;
     if (left >= 0) bparent[left] = i; else leaf_bparent[~left] = i;
     if (right >= 0) bparent[right] = i; else leaf_bparent[~right] = i;
-    if (i == 0) bparent[0] = -1;
+    if (seg_root) bparent[i] = -1;
 }
 
 // A binary node heads an octree node iff it is the root or its parent sits
@@ -396,8 +467,22 @@ __global__ void k_head_flags(const int32_t *__restrict__ bparent, const int32_t 
                              uint32_t m, uint32_t *__restrict__ flag) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
+    if (bdelta[i] < 0) {  // not an internal node (the last particle of a system)
+        flag[i] = 0u;
+        return;
+    }
     int p = bparent[i];
-    flag[i] = (i == 0 || level_of(bdelta[p]) < level_of(bdelta[i])) ? 1u : 0u;
+    flag[i] = (p < 0 || level_of(bdelta[p]) < level_of(bdelta[i])) ? 1u : 0u;
+}
+
+// Octree root of every system: the head of the binary node at the system's
+// first particle (none for a system of fewer than two particles).
+__global__ void k_sys_roots(const uint32_t *__restrict__ sys_start, const uint32_t *__restrict__ flag,
+                            const uint32_t *__restrict__ head_id, uint32_t nsys, int32_t *__restrict__ root_node) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys) return;
+    const uint32_t a = sys_start[s], b = sys_start[s + 1];
+    root_node[s] = (b - a >= 2 && flag[a]) ? (int32_t)head_id[a] : -1;
 }
 
 // Each head gathers, left to right, the exits of its same-level binary
@@ -532,15 +617,21 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
     const uint32_t n = tb.n;
     unsigned L = 0;
     if (n == 0) return cudaSuccess;
-    // root cube (+ max |v| when requested)
+    const bool multi = tb.nsys > 1;
+    // root cube (+ max |v| when requested); one per system when there are several
     k_bbox<<<tb.bbox_blocks, 256, 0, st>>>(tb.pos, tb.vel_for_max, tb.mass, n, tb.bbox_partial, tb.sc);
+    if (multi) {
+        k_bbox_systems<<<tb.nsys, 256, 0, st>>>(tb.pos, tb.mass, tb.sys_start, tb.sys_root, tb.sc);
+        L += 1;
+    }
     // keys: k1 (user order) -> key3, k2 -> key_a (sort key) and key2 (user order)
-    k_keys<<<blocks_for(n, 256), 256, 0, st>>>(tb.pos, n, tb.sc, tb.key3, tb.key_a, tb.key2, tb.idx_a);
+    k_keys<<<blocks_for(n, 256), 256, 0, st>>>(tb.pos, n, tb.sc, tb.key3, tb.key_a, tb.key2, tb.idx_a,
+                                               multi ? tb.sys_id : nullptr, tb.sys_root);
     L += 2;
     // LSD radix sort by (k1, k2): 8 passes on k2, then 8 passes on k1.
     const uint32_t nb = blocks_for(n, kSortTile);
-    auto passes = [&](uint64_t *kin, uint64_t *kout, uint32_t *iin, uint32_t *iout) {
-        for (int shift = 0; shift < 64; shift += 8) {
+    auto passes = [&](uint64_t *kin, uint64_t *kout, uint32_t *iin, uint32_t *iout, int bits = 64) {
+        for (int shift = 0; shift < bits; shift += 8) {
             k_sort_hist<<<nb, kSortThreads, 0, st>>>(kin, n, shift, tb.sort_hist, nb);
             L += 2 + scan_exclusive(tb.sort_hist, 256u * nb, tb.scan_tmp, nullptr, st);
             k_sort_scatter<<<nb, kSortThreads, 0, st>>>(kin, iin, kout, iout, n, shift, tb.sort_hist, nb);
@@ -551,15 +642,24 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
     passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b);          // result: key_a, idx_a
     k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key3, tb.idx_a, tb.key_b, n);  // k1 in that order
     passes(tb.key_b, tb.key_a, tb.idx_a, tb.idx_b);          // result: key_b (k1 sorted), idx_a
+    if (multi) {
+        // then by system (16-bit ids, 2 stable passes; result back in key_a / idx_a)
+        k_gather_sys<<<blocks_for(n, 256), 256, 0, st>>>(tb.sys_id, tb.idx_a, tb.key_a, nullptr, n);
+        passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b, 16);
+        k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key3, tb.idx_a, tb.key_b, n);  // k1 sorted
+        k_gather_sys<<<blocks_for(n, 256), 256, 0, st>>>(tb.sys_id, tb.idx_a, nullptr, tb.sys_sorted, n);
+        L += 3;
+    }
     k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key2, tb.idx_a, tb.key_a, n);  // k2 sorted
     k_gather_bodies<<<blocks_for(n, 256), 256, 0, st>>>(tb.idx_a, tb.pos, tb.mass, tb.body, n);
     L += 3;
     *launches += L;
     if (n < 2) return cudaGetLastError();
     L = 0;
+    const uint32_t *sys_sorted = multi ? tb.sys_sorted : nullptr;
     k_deep_groups<<<blocks_for(n, 256), 256, 0, st>>>(tb.key_b, tb.key_a, tb.key3, tb.idx_a, tb.body, n,
-                                                       tb.sc);
-    KeyView kv{tb.key_b, tb.key_a, tb.key3, (int)n};
+                                                       sys_sorted, tb.sys_root, tb.sc);
+    KeyView kv{tb.key_b, tb.key_a, tb.key3, (int)n, sys_sorted};
     const uint32_t m = n - 1;
     k_radix_tree<<<blocks_for(m, 256), 256, 0, st>>>(kv, tb.bleft, tb.bright, tb.bparent, tb.leaf_bparent,
                                                       tb.bdelta);
@@ -574,6 +674,11 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
                                                     m, tb.ochild, tb.ometa, tb.oparent, tb.leaf_oparent,
                                                     tb.sc);
     L += 1;
+    if (multi) {
+        k_sys_roots<<<blocks_for(tb.nsys, 256), 256, 0, st>>>(tb.sys_start, tb.head_flag, tb.head_id, tb.nsys,
+                                                               tb.sys_root_node);
+        L += 1;
+    }
     *launches += L;
     return cudaGetLastError();
 }

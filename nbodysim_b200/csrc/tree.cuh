@@ -23,6 +23,14 @@ struct TreeBuild {
     int32_t *ochild, *ometa, *oparent, *leaf_oparent;
     uint32_t *ocount;
     double4 *onode;
+    // Independent systems stored one after another (nsys > 1): each gets its
+    // own root cube and octree; none of these is read when nsys == 1.
+    uint32_t nsys;
+    const uint32_t *sys_start;   // nsys + 1 offsets (user order)
+    const uint32_t *sys_id;      // system of each particle (user order)
+    uint32_t *sys_sorted;        // system of each sorted position
+    double *sys_root;            // 4 doubles per system: center x, y, z, side
+    int32_t *sys_root_node;      // octree root of each system (-1: fewer than 2 particles)
 };
 
 // Enqueues root cube -> keys -> sort -> bodies -> radix tree -> octree.

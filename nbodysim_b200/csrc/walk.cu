@@ -323,9 +323,8 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
     Sm &s = reinterpret_cast<Sm *>(smem_raw)[wid];
     const Tree &t = a.t;
     const uint32_t n = t.n;
-    const double S = t.sc->root_side;
     const double theta = a.theta;
-    const double s_theta = S / theta;
+    const double S1 = t.sc->root_side;
     int2 *gspill = a.spill + (size_t)(blockIdx.x * kWalkWarps + wid) * a.spill_cap;
     const unsigned FULL = 0xffffffffu;
     const uint32_t lt = (1u << lane) - 1u;
@@ -336,9 +335,23 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
         g = __shfl_sync(FULL, g, 0);
         if (g >= a.n_groups) break;
 
-        const uint32_t g0 = g * 32;
+        uint32_t g0, gcount;
+        int root = 0;
+        double S = S1;
+        if (a.groups) {
+            const int4 gr = a.groups[g];
+            g0 = (uint32_t)gr.x;
+            gcount = (uint32_t)gr.y;
+            root = a.sys_root_node[gr.z];
+            S = a.sys_root[4 * (size_t)gr.z + 3];
+        } else {
+            g0 = g * 32;
+            gcount = min(32u, n - g0);
+            root = n >= 2 ? 0 : -1;
+        }
+        const double s_theta = S / theta;
         const uint32_t j = g0 + lane;
-        const bool valid = j < n;
+        const bool valid = (uint32_t)lane < gcount;
         const double4 b = t.body[valid ? j : g0];
         const uint32_t vmask = __ballot_sync(FULL, valid);
         // adjoint mode: this particle's cotangent dL/da
@@ -386,8 +399,8 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
         int top = 0, list_top = 0, max_top = 0;
         uint32_t spill_top = 0;
         bool failed = false;
-        if (n >= 2) {
-            if (lane == 0) s.stack[0] = make_int2(0, (int)vmask);
+        if (root >= 0) {
+            if (lane == 0) s.stack[0] = make_int2(root, (int)vmask);
             top = 1;
         }
         __syncwarp();

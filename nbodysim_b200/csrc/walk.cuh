@@ -35,6 +35,12 @@ struct WalkArgs {
     double *gdird;      // FP64
     double *adj_node;   // 4 doubles per internal node
     double *adj_leaf;   // 4 doubles per sorted particle
+    // Several independent systems: the work queue is a table of groups
+    // (first sorted particle, count <= 32, system); each system has its own
+    // octree root and root side. Null for a single system (groups of 32 from 0).
+    const int4 *groups;
+    const int32_t *sys_root_node;
+    const double *sys_root;     // 4 per system: center xyz, side
 };
 
 // Launch shape of the persistent walk for this device (blocks to fill every SM).
