@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU walk seconds of the sample")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--adjoint-fd", type=int, default=0,
                     help="also check the config-4 gradient against central differences on this many coordinates")
     return ap.parse_args()
@@ -218,7 +219,7 @@ def run_ours(args) -> None:
     g = nb.gen_params(gen_type=2, size=1024.0, r_sphere=100.0, rotation_magnitude=0.1, seed=0xDEADBEEF + rank)
     pos0, vel0, mass = nb.generate(args.n, g)
     params = nb.default_params(theta=args.theta, adaptive=1, min_adaptive_dt=0.00333, max_pos_change=3.0,
-                               max_vel_change=3.0, device=local)
+                               max_vel_change=3.0, device=local, autotune=1)
     eng = nb.Engine(params)
     eng._lib.nbody_set_stream(eng._h, C_void(stream.cuda_stream))
 
@@ -237,6 +238,7 @@ def run_ours(args) -> None:
         torch.cuda.synchronize()
     st = eng.stats()
     launches = st["kernel_launches"] - launches0
+    walk_shape = {"warps_per_block": st["walk_warps_per_block"], "blocks": st["walk_blocks"], "autotuned": True}
     ms_total = ev0.elapsed_time(ev1)
     inter_total = st["interactions_total"]
     if pg:
@@ -321,6 +323,11 @@ def run_ours(args) -> None:
     if not args.no_adjoint:
         adjoint = adjoint_leg(nb, torch, stream, local, args.adjoint_fd)
 
+    # ---- batched ensemble (512 systems of uneven N, one persistent walk, graphs, autotuned)
+    ensemble = None
+    if not args.no_ensemble:
+        ensemble = ensemble_leg(nb, torch, stream, local)
+
     # ---- accuracy on the initial state: vs the FP64 form (same lists) and FP64 direct sum
     acc_mixed, counts = eng.barnes_hut(pos0, mass, theta=args.theta, counts=True)
     with nb.Engine(nb.default_params(theta=args.theta, precision=nb.PRECISION_FP64, device=local)) as e64:
@@ -380,10 +387,12 @@ def run_ours(args) -> None:
         "vs_fp64_direct_sum": direct,
         "adjoint_fwd_ratio": adjoint["ratio"] if adjoint else None,
         "adjoint": adjoint,
+        "ensemble": ensemble,
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 56 * args.n,
                 "d2h_bytes_per_step": 48 * args.n},
         "gpu_launches": int(launches),
+        "walk_shape": walk_shape,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
                      "frac": achieved / peak_tf if peak_tf else None, "traffic": traffic,
                      "kernel": "k_walk (fused walk + gravity)",
@@ -447,6 +456,57 @@ def adjoint_leg(nb, torch, stream, device, fd_coords=0):
                 rel.append(abs(fd - gp[p, k]) / max(abs(fd), abs(gp[p, k]), 1e-300))
             out["fd_check"] = {"coords": fd_coords, "eps": "1e-3 relative", "median_rel": float(np.median(rel)),
                                "max_rel": float(np.max(rel)), "frac_le_1e-4": float(np.mean(np.array(rel) <= 1e-4))}
+    return out
+
+
+def ensemble_leg(nb, torch, stream, device, nsys=512, steps=100, seq_steps=10):
+    """Batched ensemble: 512 independent systems, N per system log-uniform in
+    [1024, 65536] (seeded), gen_type cycling cube/sphere/shell, masses uniform in
+    [5e10, 5e11], theta 0.5, dt 0.0333, 100 steps: one engine, one persistent
+    walk per step over all systems, steps replayed from a captured CUDA graph,
+    walk block shape autotuned. Baseline: the same systems stepped one after
+    another through one engine call each (graph replay too), seq_steps steps each."""
+    rng = np.random.default_rng(0xDEADBEEF)
+    counts = np.exp(rng.uniform(np.log(1024), np.log(65536), nsys)).astype(np.uint32)
+    parts = [nb.generate(int(c), gen_type=s % 3, size=512.0 if s % 3 == 0 else 1024.0, seed=0xDEADBEEF + s)
+             for s, c in enumerate(counts)]
+    pos = np.concatenate([p[0] for p in parts]); vel = np.concatenate([p[1] for p in parts])
+    mass = np.concatenate([p[2] for p in parts])
+    out = {"systems": nsys, "particles": int(counts.sum()), "n_min": int(counts.min()), "n_max": int(counts.max()),
+           "steps": steps, "theta": 0.5, "dt": 0.0333}
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    with nb.Engine(nb.default_params(theta=0.5, dt=0.0333, device=device, autotune=1)) as e:
+        e._lib.nbody_set_stream(e._h, C_void(stream.cuda_stream))
+        e.set_systems(counts)
+        e.set_particles(pos, vel, mass)
+        e.step(3)  # warm-up: autotune + graph capture
+        st = e.stats()
+        out["walk_shape"] = {"warps_per_block": st["walk_warps_per_block"], "blocks": st["walk_blocks"]}
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        e.step(steps)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        ms = ev[0].elapsed_time(ev[1])
+        inter = e.stats()["interactions_total"]
+    out["ensemble_ms"] = ms
+    out["ensemble_system_steps_per_s"] = nsys * steps / (ms * 1e-3)
+    out["ensemble_interactions_per_s"] = inter / (ms * 1e-3)
+    with nb.Engine(nb.default_params(theta=0.5, dt=0.0333, device=device)) as e:
+        e._lib.nbody_set_stream(e._h, C_void(stream.cuda_stream))
+        e.set_particles(parts[0][0], parts[0][1], parts[0][2])
+        e.step(2)
+        torch.cuda.synchronize()
+        ev[2].record(stream)
+        for p in parts:
+            e.set_particles(p[0], p[1], p[2])
+            e.step(seq_steps)
+        ev[3].record(stream)
+        torch.cuda.synchronize()
+        seq_ms = ev[2].elapsed_time(ev[3])
+    out["sequential_steps_per_system"] = seq_steps
+    out["sequential_system_steps_per_s"] = nsys * seq_steps / (seq_ms * 1e-3)
+    out["speedup_vs_sequential"] = out["ensemble_system_steps_per_s"] / out["sequential_system_steps_per_s"]
     return out
 
 

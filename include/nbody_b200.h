@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define NBODY_ABI_VERSION 1
+#define NBODY_ABI_VERSION 2  /* 2: nbody_params.autotune, nbody_stats walk fields */
 
 /* ---- status codes ---------------------------------------------------- */
 #define NBODY_OK 0
@@ -66,6 +66,7 @@ typedef struct nbody_params {
     double max_vel_change;  /* key `max_vel_change` (README.md:60) */
     int precision;          /* NBODY_PRECISION_* */
     int device;             /* CUDA device ordinal */
+    int autotune;           /* run nbody_autotune on the first step at each new size (default 0) */
 } nbody_params;
 
 /* Defaults of the reference's set_default (src/main.cpp:1312-1357) for the keys above;
@@ -133,6 +134,8 @@ typedef struct nbody_stats {
     uint64_t walk_decisions;     /* internal nodes the warps decided (open / accept) */
     uint64_t walk_list;          /* bodies the warps put in their interaction lists */
     uint64_t walk_near;          /* bodies taken with FP64 offsets (too close for FP32 offsets) */
+    uint32_t walk_warps_per_block; /* walk block shape in use (autotuned or default) */
+    uint32_t walk_blocks;          /* walk grid size in use (persistent blocks) */
     uint32_t tree_nodes;     /* internal nodes of the (chain-free) octree */
     uint32_t tree_depth;     /* deepest internal-node level */
     uint32_t max_stack;      /* deepest walk stack seen (entries) */
@@ -150,6 +153,10 @@ int nbody_set_timing(nbody_ctx *ctx, int enabled);
  * distinct configuration is captured on first use; a stream that cannot be
  * captured (the legacy default stream) falls back to direct launches. */
 int nbody_set_graphs(nbody_ctx *ctx, int enabled);
+/* Autotuner: times the walk on the resident state for each block shape (2, 4
+ * or 8 warps per block, all or all-but-one resident blocks per SM) and keeps
+ * the fastest for this context's precision (see nbody_stats.walk_*). */
+int nbody_autotune(nbody_ctx *ctx);
 
 typedef struct nbody_diagnostics {
     double kinetic;          /* sum 1/2 m v^2 */

@@ -47,7 +47,7 @@ class Params(C.Structure):
     _fields_ = [
         ("theta", C.c_double), ("dt", C.c_double), ("damping", C.c_int), ("adaptive", C.c_int),
         ("min_adaptive_dt", C.c_double), ("max_pos_change", C.c_double), ("max_vel_change", C.c_double),
-        ("precision", C.c_int), ("device", C.c_int),
+        ("precision", C.c_int), ("device", C.c_int), ("autotune", C.c_int),
     ]
 
 
@@ -66,6 +66,7 @@ class Stats(C.Structure):
         ("interactions", C.c_uint64), ("interactions_total", C.c_uint64), ("kernel_launches", C.c_uint64),
         ("walk_entries", C.c_uint64), ("walk_tiles", C.c_uint64), ("walk_decisions", C.c_uint64),
         ("walk_list", C.c_uint64), ("walk_near", C.c_uint64),
+        ("walk_warps_per_block", C.c_uint32), ("walk_blocks", C.c_uint32),
         ("tree_nodes", C.c_uint32), ("tree_depth", C.c_uint32),
         ("max_stack", C.c_uint32), ("fallback_tests", C.c_uint32), ("last_dt", C.c_double),
         ("root_center", C.c_double * 3), ("root_side", C.c_double),
@@ -114,6 +115,7 @@ _SIGS = {
     "nbody_get_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "nbody_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "nbody_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
+    "nbody_autotune": (C.c_int, [C.c_void_p]),
     "nbody_get_diagnostics": (C.c_int, [C.c_void_p, C.POINTER(Diagnostics)]),
     "nbody_default_gen_params": (None, [C.POINTER(GenParams)]),
     "nbody_generate": (C.c_int, [C.POINTER(GenParams), C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -250,6 +252,12 @@ class Engine:
         for k, v in kw.items():
             setattr(self.params, k, v)
         _check(self._lib.nbody_set_params(self._h, C.byref(self.params)))
+
+    def autotune(self) -> dict:
+        """Picks the fastest walk block shape on the resident state."""
+        _check(self._lib.nbody_autotune(self._h))
+        s = self.stats()
+        return {"warps_per_block": s["walk_warps_per_block"], "blocks": s["walk_blocks"]}
 
     def set_graphs(self, on: bool = True) -> None:
         _check(self._lib.nbody_set_graphs(self._h, int(on)))

@@ -74,6 +74,8 @@ struct nbody_ctx {
     cudaEvent_t ev[5] = {};
     nbody_stats stats{};
     unsigned long long launches = 0;  // kernels enqueued by this context
+    unsigned max_walk_warps = 0;      // spill regions allocated
+    std::vector<unsigned char> tuned_key;  // configuration the autotuner last ran for
     // adjoint state (allocated on first use)
     void *adj_arena = nullptr;
     size_t adj_bytes = 0;
@@ -127,9 +129,7 @@ int reserve(nbody_ctx *c, uint32_t n) {
     const size_t N = cap;
     const size_t sort_blocks = (N + 4095) / 4096;
     const size_t scan_tiles = (256 * sort_blocks + 4095) / 4096 + (N + 4095) / 4096 + 8;
-    const size_t spill_entries = (size_t)(c->wl_mixed.blocks > c->wl_fp64.blocks ? c->wl_mixed.blocks
-                                                                                   : c->wl_fp64.blocks) *
-                                 kWalkWarps * kSpillCap;
+    const size_t spill_entries = (size_t)c->max_walk_warps * kSpillCap;
     struct Piece { void **dst; size_t bytes; };
     TreeBuild &tb = c->tb;
     Piece pieces[] = {
@@ -188,6 +188,11 @@ int check_status(nbody_ctx *c) {
     s.walk_list = h.walk_list;
     s.walk_near = h.walk_near;
     s.kernel_launches = c->launches;
+    {
+        const WalkLaunch &w = c->p.precision == NBODY_PRECISION_FP64 ? c->wl_fp64 : c->wl_mixed;
+        s.walk_warps_per_block = w.warps;
+        s.walk_blocks = w.blocks;
+    }
     s.tree_nodes = h.n_onodes;
     s.tree_depth = h.depth;
     s.max_stack = h.max_stack;
@@ -223,7 +228,8 @@ void ev(nbody_ctx *c, int k) {
 
 // One force pass on the resident pos/mass: tree, COM, walk. Asynchronous.
 int force_pass(nbody_ctx *c, int damping, double theta, bool fp64, bool want_vmax, bool track_amax,
-               bool want_counts, bool want_pot, const double *pos = nullptr, bool adjoint = false) {
+               bool want_counts, bool want_pot, const double *pos = nullptr, bool adjoint = false,
+               const WalkLaunch *shape = nullptr) {
     const uint32_t n = c->n;
     unsigned launches = 1;
     NB_CUDA(launch_reset_pass(c->sc, c->stream));
@@ -274,7 +280,7 @@ int force_pass(nbody_ctx *c, int damping, double theta, bool fp64, bool want_vma
         NB_CUDA(cudaMemsetAsync(c->adj_leaf, 0, 32 * (size_t)n, c->stream));
     }
     if (n > 0) {
-        NB_CUDA(launch_walk(a, fp64, fp64 ? c->wl_fp64 : c->wl_mixed, c->stream));
+        NB_CUDA(launch_walk(a, fp64, shape ? *shape : fp64 ? c->wl_fp64 : c->wl_mixed, c->stream));
         launches++;
     }
     c->launches += launches;
@@ -467,6 +473,72 @@ int step_on(nbody_ctx *c, double *pos, double *vel, bool fp64) {
     return NBODY_OK;
 }
 
+// ---- autotuner ----------------------------------------------------------------
+// Times the walk on the resident state for every block shape (2, 4 or 8 warps
+// per block; all or all-but-one resident blocks per SM) and keeps the fastest
+// for this context's precision. Tree and COM are rebuilt per candidate so each
+// walk starts from the same state; only the walk is timed (CUDA events, best of 3).
+std::vector<unsigned char> tune_key(nbody_ctx *c) {
+    struct K { uint32_t n_bucket, nsys; int precision, damping; double theta; } k;
+    std::memset(&k, 0, sizeof k);
+    uint32_t b = 1;
+    while (b < c->n) b <<= 1;
+    k.n_bucket = b; k.nsys = c->nsys; k.precision = c->p.precision; k.damping = c->p.damping; k.theta = c->p.theta;
+    const unsigned char *p = (const unsigned char *)&k;
+    return std::vector<unsigned char>(p, p + sizeof k);
+}
+
+int autotune(nbody_ctx *c) {
+    const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
+    const int saved_timing = c->timing;
+    c->timing = 1;
+    WalkLaunch best = fp64 ? c->wl_fp64 : c->wl_mixed;
+    float best_ms = 1e30f;
+    int rc = NBODY_OK;
+    for (unsigned w : {2u, 4u, 8u}) {
+        int maxb = 0;
+        if (walk_max_blocks_per_sm(fp64, w, &maxb) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        for (int bps = maxb; bps >= 1 && bps >= maxb - 1; bps--) {
+            WalkLaunch shape{};
+            if (walk_launch_shape(fp64, c->p.device, w, (unsigned)bps, &shape) != cudaSuccess) {
+                cudaGetLastError();
+                continue;
+            }
+            if ((size_t)shape.blocks * shape.warps > c->max_walk_warps) continue;
+            float ms = 1e30f;
+            for (int r = 0; r < 3 && rc == NBODY_OK; r++) {
+                rc = force_pass(c, c->p.damping, c->p.theta, fp64, false, false, false, false, nullptr, false, &shape);
+                if (rc) break;
+                if ((rc = copy_scalars_back(c))) break;
+                if ((rc = check_status(c))) break;
+                ms = std::min(ms, c->stats.ms_walk);
+            }
+            if (rc) break;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = shape;
+            }
+        }
+        if (rc) break;
+    }
+    c->timing = saved_timing;
+    if (rc) return rc;
+    if (fp64) c->wl_fp64 = best;
+    else c->wl_mixed = best;
+    drop_graphs(c);
+    c->tuned_key = tune_key(c);
+    return NBODY_OK;
+}
+
+int maybe_autotune(nbody_ctx *c) {
+    if (!c->p.autotune || c->n < 2) return NBODY_OK;
+    if (tune_key(c) == c->tuned_key) return NBODY_OK;
+    return autotune(c);
+}
+
 // Runs `body` through the graph cached at slot i (capturing it on first use).
 template <class F>
 int run_cached(nbody_ctx *c, std::vector<cudaGraphExec_t> &execs, std::vector<unsigned> &launches, uint32_t i,
@@ -508,6 +580,7 @@ void nbody_default_params(nbody_params *p) {
     p->max_vel_change = 3;         // README.md:60
     p->precision = NBODY_PRECISION_MIXED;
     p->device = 0;
+    p->autotune = 0;
 }
 
 int nbody_create(const nbody_params *p, nbody_ctx **out) {
@@ -539,10 +612,20 @@ int nbody_create(const nbody_params *p, nbody_ctx **out) {
     std::memset(c->hsc, 0, sizeof(DevScalars));
     for (auto &e : c->ev)
         if (cudaEventCreate(&e) != cudaSuccess) return cleanup(fail(NBODY_ERR_CUDA, "event%s"));
-    if (walk_launch_shape(false, p->device, &c->wl_mixed) != cudaSuccess ||
-        walk_launch_shape(true, p->device, &c->wl_fp64) != cudaSuccess)
+    if (walk_launch_shape(false, p->device, kWalkWarps, 0, &c->wl_mixed) != cudaSuccess ||
+        walk_launch_shape(true, p->device, kWalkWarps, 0, &c->wl_fp64) != cudaSuccess)
         return cleanup(fail(NBODY_ERR_CUDA, "walk kernel configuration failed (%s)",
                             cudaGetErrorString(cudaGetLastError())));
+    // spill regions for the largest resident warp count any tuned shape can have
+    for (unsigned w : {2u, 4u, 8u})
+        for (int fp = 0; fp < 2; fp++) {
+            int mb = 0;
+            if (walk_max_blocks_per_sm(fp != 0, w, &mb) != cudaSuccess) {
+                cudaGetLastError();
+                continue;
+            }
+            c->max_walk_warps = std::max(c->max_walk_warps, (unsigned)(prop.multiProcessorCount * mb * (int)w));
+        }
     *out = c;
     return NBODY_OK;
 }
@@ -582,6 +665,15 @@ int nbody_set_stream(nbody_ctx *c, void *stream) {
     c->stream = (cudaStream_t)stream;
     c->own_stream = false;
     return NBODY_OK;
+}
+
+int nbody_autotune(nbody_ctx *c) {
+    CTX_OR_FAIL(c);
+    if (!c->have_state) return fail(NBODY_ERR_STATE, "no particles set%s");
+    if (c->n < 2) return NBODY_OK;
+    int rc = begin_call(c);
+    if (rc) return rc;
+    return autotune(c);
 }
 
 int nbody_set_graphs(nbody_ctx *c, int enabled) {
@@ -726,6 +818,7 @@ int nbody_step(nbody_ctx *c, uint32_t nsteps) {
     if (c->n == 0 || nsteps == 0) return NBODY_OK;
     int rc = begin_call(c);
     if (rc) return rc;
+    if ((rc = maybe_autotune(c))) return rc;
     rc = run_steps(c, nsteps);
     if (rc) return rc;
     if ((rc = copy_scalars_back(c))) return rc;
@@ -837,6 +930,7 @@ int nbody_forward_checkpointed(nbody_ctx *c, uint32_t nsteps, uint32_t every) {
     int rc = reserve_adjoint(c, c->n, every, nseg);
     if (rc) return rc;
     if ((rc = begin_call(c))) return rc;
+    if ((rc = maybe_autotune(c))) return rc;
     const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
     const size_t N3 = 3 * (size_t)c->n;
     (void)fp64;

@@ -316,7 +316,7 @@ __device__ inline void flush_list(Sm &s, int count, int lane, const WalkArgs &a,
 }
 
 template <bool kFp64, bool kDamp, bool kPot, bool kAdj>
-__global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
+__global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using Sm = WarpSmem<kFp64>;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(kWalkWarps * 32) k_walk(WalkArgs a) {
     const uint32_t n = t.n;
     const double theta = a.theta;
     const double S1 = t.sc->root_side;
-    int2 *gspill = a.spill + (size_t)(blockIdx.x * kWalkWarps + wid) * a.spill_cap;
+    int2 *gspill = a.spill + (size_t)(blockIdx.x * (blockDim.x >> 5) + wid) * a.spill_cap;
     const unsigned FULL = 0xffffffffu;
     const uint32_t lt = (1u << lane) - 1u;
 
@@ -680,37 +680,48 @@ const void *any_walk_kernel(bool fp64, bool adj, int damping, bool pot) {
 
 }  // namespace
 
-cudaError_t walk_launch_shape(bool fp64, int device, WalkLaunch *out) {
-    const size_t smem = (fp64 ? sizeof(WarpSmem<true>) : sizeof(WarpSmem<false>)) * kWalkWarps;
+cudaError_t walk_max_blocks_per_sm(bool fp64, unsigned warps, int *out) {
+    const size_t smem = (fp64 ? sizeof(WarpSmem<true>) : sizeof(WarpSmem<false>)) * warps;
     int minblocks = 1 << 30;
     for (int adj = 0; adj < 2; adj++)
         for (int damp = 0; damp < 2; damp++)
             for (int pot = 0; pot < 2 - adj; pot++) {
                 const void *k = any_walk_kernel(fp64, adj, damp, pot);
-                cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)(sizeof(WarpSmem<true>) * kWalkMaxWarps));
                 if (e != cudaSuccess) return e;
                 int nb = 0;
-                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kWalkWarps * 32, smem);
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, (int)warps * 32, smem);
                 if (e != cudaSuccess) return e;
                 minblocks = nb < minblocks ? nb : minblocks;
             }
-    int sms = 0;
-    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    *out = minblocks;
+    return cudaSuccess;
+}
+
+cudaError_t walk_launch_shape(bool fp64, int device, unsigned warps, unsigned blocks_per_sm, WalkLaunch *out) {
+    int maxb = 0;
+    cudaError_t e = walk_max_blocks_per_sm(fp64, warps, &maxb);
     if (e != cudaSuccess) return e;
-    if (minblocks < 1) minblocks = 1;
-    out->blocks = (unsigned)(sms * minblocks);
-    out->smem = smem;
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    if (maxb < 1) maxb = 1;
+    const int per_sm = blocks_per_sm ? (int)blocks_per_sm < maxb ? (int)blocks_per_sm : maxb : maxb;
+    out->blocks = (unsigned)(sms * per_sm);
+    out->warps = warps;
+    out->smem = (fp64 ? sizeof(WarpSmem<true>) : sizeof(WarpSmem<false>)) * warps;
     return cudaSuccess;
 }
 
 cudaError_t launch_walk(const WalkArgs &a, bool fp64, const WalkLaunch &l, cudaStream_t st) {
     const void *k = any_walk_kernel(fp64, a.adjoint != 0, a.damping, a.pot != nullptr);
     unsigned blocks = l.blocks;
-    const unsigned need = (a.n_groups + kWalkWarps - 1) / kWalkWarps;
+    const unsigned need = (a.n_groups + l.warps - 1) / l.warps;
     if (need < blocks) blocks = need ? need : 1;
     WalkArgs args = a;
     void *params[] = {&args};
-    return cudaLaunchKernel(k, dim3(blocks), dim3(kWalkWarps * 32), params, l.smem, st);
+    return cudaLaunchKernel(k, dim3(blocks), dim3(l.warps * 32), params, l.smem, st);
 }
 
 }  // namespace nbody

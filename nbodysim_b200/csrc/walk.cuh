@@ -5,7 +5,8 @@
 
 namespace nbody {
 
-constexpr int kWalkWarps = 4;       // warps per block
+constexpr int kWalkWarps = 4;       // default warps per block (the autotuner may pick 2 or 8)
+constexpr int kWalkMaxWarps = 8;    // largest block the walk kernel is compiled for
 constexpr int kStackCap = 768;      // shared-memory stack entries per warp
 constexpr int kSpillChunk = kStackCap / 2;
 constexpr int kListFlush = 32;      // force pass once the interaction list holds this many
@@ -43,12 +44,17 @@ struct WalkArgs {
     const double *sys_root;     // 4 per system: center xyz, side
 };
 
-// Launch shape of the persistent walk for this device (blocks to fill every SM).
+// Launch shape of the persistent walk: `warps` per block, `blocks` in the grid
+// (a whole number of resident blocks per SM), `smem` bytes per block.
 struct WalkLaunch {
     unsigned blocks;
+    unsigned warps;
     size_t smem;
 };
-cudaError_t walk_launch_shape(bool fp64, int device, WalkLaunch *out);
+// blocks_per_sm = 0: as many as fit. Returns the shape for that block size.
+cudaError_t walk_launch_shape(bool fp64, int device, unsigned warps, unsigned blocks_per_sm, WalkLaunch *out);
+// Resident blocks per SM that fit for `warps` per block (all walk variants).
+cudaError_t walk_max_blocks_per_sm(bool fp64, unsigned warps, int *out);
 cudaError_t launch_walk(const WalkArgs &a, bool fp64, const WalkLaunch &l, cudaStream_t st);
 
 }  // namespace nbody

@@ -95,3 +95,21 @@ def test_set_systems_validation(nb):
         e.set_systems([16])
         e.set_particles(pos, vel, mass)
         e.step(1)
+
+
+def test_autotune_picks_a_valid_shape_and_keeps_results(nb):
+    pos, vel, mass = nb.generate(30000, gen_type=2, size=1024.0)
+    with nb.Engine() as e:
+        e.set_particles(pos, vel, mass)
+        e.compute_forces()
+        _, _, a0 = e.get_particles(acc=True)
+        shape = e.autotune()
+        assert shape["warps_per_block"] in (2, 4, 8) and shape["blocks"] > 0
+        e.compute_forces()
+        _, _, a1 = e.get_particles(acc=True)
+    # the block shape changes which warp runs which group, never a group's arithmetic
+    assert np.array_equal(a0, a1)
+    with nb.Engine(autotune=1) as e:
+        e.set_particles(pos, vel, mass)
+        e.step(2)
+        assert e.stats()["walk_warps_per_block"] in (2, 4, 8)
