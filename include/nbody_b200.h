@@ -153,8 +153,8 @@ int nbody_set_timing(nbody_ctx *ctx, int enabled);
  * distinct configuration is captured on first use; a stream that cannot be
  * captured (the legacy default stream) falls back to direct launches. */
 int nbody_set_graphs(nbody_ctx *ctx, int enabled);
-/* Autotuner: times the walk on the resident state for each block shape (2, 4
- * or 8 warps per block, all or all-but-one resident blocks per SM) and keeps
+/* Autotuner: times the walk on the resident state for each block shape (1, 2
+ * or 4 warps per block, all or all-but-one resident blocks per SM) and keeps
  * the fastest for this context's precision (see nbody_stats.walk_*). */
 int nbody_autotune(nbody_ctx *ctx);
 

@@ -474,7 +474,7 @@ int step_on(nbody_ctx *c, double *pos, double *vel, bool fp64) {
 }
 
 // ---- autotuner ----------------------------------------------------------------
-// Times the walk on the resident state for every block shape (2, 4 or 8 warps
+// Times the walk on the resident state for every block shape (1, 2 or 4 warps
 // per block; all or all-but-one resident blocks per SM) and keeps the fastest
 // for this context's precision. Tree and COM are rebuilt per candidate so each
 // walk starts from the same state; only the walk is timed (CUDA events, best of 3).
@@ -495,7 +495,7 @@ int autotune(nbody_ctx *c) {
     WalkLaunch best = fp64 ? c->wl_fp64 : c->wl_mixed;
     float best_ms = 1e30f;
     int rc = NBODY_OK;
-    for (unsigned w : {2u, 4u, 8u}) {
+    for (unsigned w : {1u, 2u, 4u}) {
         int maxb = 0;
         if (walk_max_blocks_per_sm(fp64, w, &maxb) != cudaSuccess) {
             cudaGetLastError();
@@ -617,7 +617,7 @@ int nbody_create(const nbody_params *p, nbody_ctx **out) {
         return cleanup(fail(NBODY_ERR_CUDA, "walk kernel configuration failed (%s)",
                             cudaGetErrorString(cudaGetLastError())));
     // spill regions for the largest resident warp count any tuned shape can have
-    for (unsigned w : {2u, 4u, 8u})
+    for (unsigned w : {1u, 2u, 4u})
         for (int fp = 0; fp < 2; fp++) {
             int mb = 0;
             if (walk_max_blocks_per_sm(fp != 0, w, &mb) != cudaSuccess) {

@@ -106,38 +106,70 @@ __device__ inline void spill_in(Sm &s, int &top, uint32_t &spill_top, const int2
 
 // Gravity of the listed bodies on each lane's particle: a lane takes an entry
 // iff its bit is set in the entry's mask.
+template <bool kDamp>
+__device__ inline float pair_f32(float dx, float dy, float dz, float gm, float &inv) {
+    const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    inv = rsqrtf(r2);
+    if constexpr (kDamp) {
+        const float r = r2 * inv;
+        return gm * inv / (r2 + expf(-r));
+    } else {
+        return gm * inv * (inv * inv);
+    }
+}
+
+// The masked force loop: every lane computes every entry, a lane adds it iff
+// its bit (`bit`) is set in the entry's mask. Entries go in pairs into two
+// accumulator sets, which breaks the dependence chain of the sums.
 template <bool kDamp, bool kPot>
-__device__ inline void force_list_f32(const float4 *lc, const uint32_t *lm, int count, int lane, float px,
-                                      float py, float pz, float &ax, float &ay, float &az, float &pot,
-                                      uint32_t &cnt) {
-#pragma unroll 4
-    for (int k = 0; k < count; k++) {
-        const float4 c = lc[k];
-        const bool take = (lm[k] >> lane) & 1u;
-        const float dx = c.x - px, dy = c.y - py, dz = c.z - pz;
-        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-        const float inv = rsqrtf(r2);
-        float f;
-        if constexpr (kDamp) {
-            const float r = r2 * inv;
-            f = c.w * inv / (r2 + expf(-r));
-        } else {
-            f = c.w * inv * (inv * inv);
+__device__ inline void force_list_f32(const float4 *lc, const uint32_t *lm, int count, uint32_t bit, float px,
+                                      float py, float pz, float &ax, float &ay, float &az, float &pot) {
+    float bx = 0.f, by = 0.f, bz = 0.f, bp = 0.f;
+    int k = 0;
+#pragma unroll 2
+    for (; k + 1 < count; k += 2) {
+        const float4 c0 = lc[k], c1 = lc[k + 1];
+        const uint32_t m0 = lm[k], m1 = lm[k + 1];
+        const float dx0 = c0.x - px, dy0 = c0.y - py, dz0 = c0.z - pz;
+        const float dx1 = c1.x - px, dy1 = c1.y - py, dz1 = c1.z - pz;
+        float inv0, inv1;
+        const float f0 = pair_f32<kDamp>(dx0, dy0, dz0, c0.w, inv0);
+        const float f1 = pair_f32<kDamp>(dx1, dy1, dz1, c1.w, inv1);
+        if (m0 & bit) {
+            ax = fmaf(f0, dx0, ax); ay = fmaf(f0, dy0, ay); az = fmaf(f0, dz0, az);
+            if constexpr (kPot) pot = fmaf(c0.w, inv0, pot);
         }
-        if (take) {
-            ax = fmaf(f, dx, ax); ay = fmaf(f, dy, ay); az = fmaf(f, dz, az);
-            if constexpr (kPot) pot = fmaf(c.w, inv, pot);
-            cnt++;
+        if (m1 & bit) {
+            bx = fmaf(f1, dx1, bx); by = fmaf(f1, dy1, by); bz = fmaf(f1, dz1, bz);
+            if constexpr (kPot) bp = fmaf(c1.w, inv1, bp);
         }
     }
+    if (k < count) {
+        const float4 c = lc[k];
+        const float dx = c.x - px, dy = c.y - py, dz = c.z - pz;
+        float inv;
+        const float f = pair_f32<kDamp>(dx, dy, dz, c.w, inv);
+        if (lm[k] & bit) {
+            ax = fmaf(f, dx, ax); ay = fmaf(f, dy, ay); az = fmaf(f, dz, az);
+            if constexpr (kPot) pot = fmaf(c.w, inv, pot);
+        }
+    }
+    ax += bx; ay += by; az += bz;
+    if constexpr (kPot) pot += bp;
+}
+
+// Per-particle accepted-body counts of a list (only when counts are requested).
+__device__ inline uint32_t count_list(const uint32_t *lm, int count, uint32_t bit) {
+    uint32_t c = 0;
+    for (int k = 0; k < count; k++) c += (lm[k] & bit) ? 1u : 0u;
+    return c;
 }
 
 // Bodies too close to the group's box for FP32 offsets: each lane forms its
 // offset in FP64 from absolute coordinates, then runs the FP32 pair force.
 template <bool kDamp, bool kPot>
 __device__ inline void force_near_f32(const double4 *nc, const uint32_t *nm, int count, int lane, double bx,
-                                      double by, double bz, float &ax, float &ay, float &az, float &pot,
-                                      uint32_t &cnt) {
+                                      double by, double bz, float &ax, float &ay, float &az, float &pot) {
     for (int k = 0; k < count; k++) {
         if (!((nm[k] >> lane) & 1u)) continue;
         const double4 c = nc[k];
@@ -154,7 +186,6 @@ __device__ inline void force_near_f32(const double4 *nc, const uint32_t *nm, int
         }
         ax = fmaf(f, dx, ax); ay = fmaf(f, dy, ay); az = fmaf(f, dz, az);
         if constexpr (kPot) pot = fmaf(gm, inv, pot);
-        cnt++;
     }
 }
 
@@ -220,7 +251,7 @@ __device__ inline void scatter_adj(double *adj_node, double *adj_leaf, int ref, 
 template <bool kDamp>
 __device__ inline void adj_list_f32(const float4 *lc, const uint32_t *lm, const int *lr, int count, int lane,
                                     float px, float py, float pz, float lax, float lay, float laz, float &gx,
-                                    float &gy, float &gz, double *adj_node, double *adj_leaf, uint32_t &cnt) {
+                                    float &gy, float &gz, double *adj_node, double *adj_leaf) {
     for (int k = 0; k < count; k++) {
         const float4 c = lc[k];
         const bool take = (lm[k] >> lane) & 1u;
@@ -229,7 +260,6 @@ __device__ inline void adj_list_f32(const float4 *lc, const uint32_t *lm, const 
         float vx, vy, vz, mt;
         pair_adjoint<kDamp, float>(dx, dy, dz, r2, c.w, lax, lay, laz, vx, vy, vz, mt);
         if (!take) vx = vy = vz = mt = 0.f;
-        else cnt++;
         gx -= vx; gy -= vy; gz -= vz;
         const float z = warp_sum4(vx, vy, vz, mt, lane);
         scatter_adj(adj_node, adj_leaf, lr[k], (double)z, lane);
@@ -239,7 +269,7 @@ __device__ inline void adj_list_f32(const float4 *lc, const uint32_t *lm, const 
 template <bool kDamp>
 __device__ inline void adj_near_f32(const double4 *nc, const uint32_t *nm, const int *nr, int count, int lane,
                                     double bx, double by, double bz, float lax, float lay, float laz, float &gx,
-                                    float &gy, float &gz, double *adj_node, double *adj_leaf, uint32_t &cnt) {
+                                    float &gy, float &gz, double *adj_node, double *adj_leaf) {
     for (int k = 0; k < count; k++) {
         const double4 c = nc[k];
         const bool take = (nm[k] >> lane) & 1u;
@@ -248,7 +278,6 @@ __device__ inline void adj_near_f32(const double4 *nc, const uint32_t *nm, const
             const float dx = (float)(c.x - bx), dy = (float)(c.y - by), dz = (float)(c.z - bz);
             const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
             pair_adjoint<kDamp, float>(dx, dy, dz, r2, (float)c.w, lax, lay, laz, vx, vy, vz, mt);
-            cnt++;
         }
         gx -= vx; gy -= vy; gz -= vz;
         const float z = warp_sum4(vx, vy, vz, mt, lane);
@@ -259,7 +288,7 @@ __device__ inline void adj_near_f32(const double4 *nc, const uint32_t *nm, const
 template <bool kDamp>
 __device__ inline void adj_list_f64(const double4 *lc, const uint32_t *lm, const int *lr, int count, int lane,
                                     double bx, double by, double bz, double lax, double lay, double laz, double &gx,
-                                    double &gy, double &gz, double *adj_node, double *adj_leaf, uint32_t &cnt) {
+                                    double &gy, double &gz, double *adj_node, double *adj_leaf) {
     for (int k = 0; k < count; k++) {
         const double4 c = lc[k];
         const bool take = (lm[k] >> lane) & 1u;
@@ -268,7 +297,6 @@ __device__ inline void adj_list_f64(const double4 *lc, const uint32_t *lm, const
             const double dx = c.x - bx, dy = c.y - by, dz = c.z - bz;
             const double r2 = dx * dx + dy * dy + dz * dz;
             pair_adjoint<kDamp, double>(dx, dy, dz, r2, c.w, lax, lay, laz, vx, vy, vz, mt);
-            cnt++;
         }
         gx -= vx; gy -= vy; gz -= vz;
         const double z = warp_sum4(vx, vy, vz, mt, lane);
@@ -278,8 +306,7 @@ __device__ inline void adj_list_f64(const double4 *lc, const uint32_t *lm, const
 
 template <bool kDamp, bool kPot>
 __device__ inline void force_list_f64(const double4 *lc, const uint32_t *lm, int count, int lane, double bx,
-                                      double by, double bz, double &ax, double &ay, double &az, double &pot,
-                                      uint32_t &cnt) {
+                                      double by, double bz, double &ax, double &ay, double &az, double &pot) {
 #pragma unroll 2
     for (int k = 0; k < count; k++) {
         const uint32_t m = lm[k];
@@ -294,7 +321,6 @@ __device__ inline void force_list_f64(const double4 *lc, const uint32_t *lm, int
         else f = c.w * inv * inv * inv;
         ax = fma(f, dx, ax); ay = fma(f, dy, ay); az = fma(f, dz, az);
         if constexpr (kPot) pot += c.w * inv;
-        cnt++;
     }
 }
 
@@ -302,17 +328,19 @@ template <bool kFp64, bool kDamp, bool kPot, bool kAdj, class Sm>
 __device__ inline void flush_list(Sm &s, int count, int lane, const WalkArgs &a, const double4 &b, float px, float py,
                                   float pz, double lax, double lay, double laz, float &fax, float &fay, float &faz,
                                   float &fpot, double &dax, double &day, double &daz, double &dpot, uint32_t &cnt) {
+    const uint32_t bit = 1u << lane;
     if constexpr (kAdj) {
         if constexpr (kFp64)
             adj_list_f64<kDamp>(s.lc, s.lm, s.lr, count, lane, b.x, b.y, b.z, lax, lay, laz, dax, day, daz, a.adj_node,
-                                a.adj_leaf, cnt);
+                                a.adj_leaf);
         else
             adj_list_f32<kDamp>(s.lc, s.lm, s.lr, count, lane, px, py, pz, (float)lax, (float)lay, (float)laz, fax, fay,
-                                faz, a.adj_node, a.adj_leaf, cnt);
+                                faz, a.adj_node, a.adj_leaf);
     } else {
-        if constexpr (kFp64) force_list_f64<kDamp, kPot>(s.lc, s.lm, count, lane, b.x, b.y, b.z, dax, day, daz, dpot, cnt);
-        else force_list_f32<kDamp, kPot>(s.lc, s.lm, count, lane, px, py, pz, fax, fay, faz, fpot, cnt);
+        if constexpr (kFp64) force_list_f64<kDamp, kPot>(s.lc, s.lm, count, lane, b.x, b.y, b.z, dax, day, daz, dpot);
+        else force_list_f32<kDamp, kPot>(s.lc, s.lm, count, bit, px, py, pz, fax, fay, faz, fpot);
     }
+    if (a.counts) cnt += count_list(s.lm, count, bit);
 }
 
 template <bool kFp64, bool kDamp, bool kPot, bool kAdj>
@@ -395,7 +423,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
 
         float fax = 0.f, fay = 0.f, faz = 0.f, fpot = 0.f;
         double dax = 0.0, day = 0.0, daz = 0.0, dpot = 0.0;
-        uint32_t cnt = 0, nfallback = 0, nentries = 0, ntiles = 0, ndecide = 0, nlist = 0, nnear = 0;
+        uint32_t cnt = 0, nint = 0, nfallback = 0, nentries = 0, ntiles = 0, ndecide = 0, nlist = 0, nnear = 0;
         int top = 0, list_top = 0, max_top = 0;
         uint32_t spill_top = 0;
         bool failed = false;
@@ -544,6 +572,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
             // extent would lose too many bits in FP32 offsets (and could give a
             // zero r^2); it goes to the near list, whose offsets are taken in FP64.
             const uint32_t accm = reach & ~my_open;
+            nint += __popc(accm);
             bool near = false;
             if constexpr (!kFp64) {
                 if (accm) {
@@ -574,9 +603,10 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                     __syncwarp();
                     if constexpr (kAdj)
                         adj_near_f32<kDamp>(s.nc, s.nm, s.nr, __popc(nmk), lane, b.x, b.y, b.z, (float)lax, (float)lay,
-                                            (float)laz, fax, fay, faz, a.adj_node, a.adj_leaf, cnt);
+                                            (float)laz, fax, fay, faz, a.adj_node, a.adj_leaf);
                     else
-                        force_near_f32<kDamp, kPot>(s.nc, s.nm, __popc(nmk), lane, b.x, b.y, b.z, fax, fay, faz, fpot, cnt);
+                        force_near_f32<kDamp, kPot>(s.nc, s.nm, __popc(nmk), lane, b.x, b.y, b.z, fax, fay, faz, fpot);
+                    if (a.counts) cnt += count_list(s.nm, __popc(nmk), 1u << lane);
                     nnear += __popc(nmk);
                     __syncwarp();
                 }
@@ -641,7 +671,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                 if (a.pot) a.pot[ui] = kFp64 ? -dpot : -(double)fpot;
             }
         }
-        unsigned long long wc = valid ? cnt : 0u;
+        unsigned long long wc = nint;
         for (int o = 16; o; o >>= 1) wc += __shfl_xor_sync(FULL, wc, o);
         uint32_t wf = nfallback;
         for (int o = 16; o; o >>= 1) wf += __shfl_xor_sync(FULL, wf, o);

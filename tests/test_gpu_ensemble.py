@@ -104,7 +104,7 @@ def test_autotune_picks_a_valid_shape_and_keeps_results(nb):
         e.compute_forces()
         _, _, a0 = e.get_particles(acc=True)
         shape = e.autotune()
-        assert shape["warps_per_block"] in (2, 4, 8) and shape["blocks"] > 0
+        assert shape["warps_per_block"] in (1, 2, 4) and shape["blocks"] > 0
         e.compute_forces()
         _, _, a1 = e.get_particles(acc=True)
     # the block shape changes which warp runs which group, never a group's arithmetic
@@ -112,4 +112,4 @@ def test_autotune_picks_a_valid_shape_and_keeps_results(nb):
     with nb.Engine(autotune=1) as e:
         e.set_particles(pos, vel, mass)
         e.step(2)
-        assert e.stats()["walk_warps_per_block"] in (2, 4, 8)
+        assert e.stats()["walk_warps_per_block"] in (1, 2, 4)
