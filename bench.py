@@ -205,6 +205,7 @@ def run_ours(args) -> None:
     import torch
     import nbodysim_b200 as nb
     from nbodysim_b200 import build as nbbuild
+    from nbodysim_b200.replicas import job_totals
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -241,15 +242,7 @@ def run_ours(args) -> None:
     walk_shape = {"warps_per_block": st["walk_warps_per_block"], "blocks": st["walk_blocks"], "autotuned": True}
     ms_total = ev0.elapsed_time(ev1)
     inter_total = st["interactions_total"]
-    if pg:
-        t = torch.tensor([ms_total], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms_total = float(t.item())
-        it = torch.tensor([float(inter_total)], device="cuda", dtype=torch.float64)
-        pg.all_reduce(it)
-        inter_all = float(it.item())
-    else:
-        inter_all = float(inter_total)
+    ms_total, inter_all = job_totals(pg, "cuda", ms_total, inter_total)
     ms_step = ms_total / args.steps
     value = inter_all / (ms_total * 1e-3)
     steps_per_s = 1e3 / ms_step
@@ -287,13 +280,7 @@ def run_ours(args) -> None:
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    if pg:
-        t = torch.tensor([e2e_ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-        it = torch.tensor([float(inter_e2e)], device="cuda", dtype=torch.float64)
-        pg.all_reduce(it)
-        inter_e2e = float(it.item())
+    e2e_ms, inter_e2e = job_totals(pg, "cuda", e2e_ms, inter_e2e)
     e2e_value = float(inter_e2e) / (e2e_ms * 1e-3)
 
     if rank != 0:
