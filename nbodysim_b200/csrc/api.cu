@@ -20,6 +20,7 @@
 #include "../../include/nbody_b200.h"
 #include "step.cuh"
 #include "tree.cuh"
+#include "sort.cuh"
 #include "walk.cuh"
 
 using namespace nbody;
@@ -138,7 +139,7 @@ int reserve(nbody_ctx *c, uint32_t n) {
         {(void **)&c->pot, 8 * N},
         {(void **)&tb.key_a, 8 * N}, {(void **)&tb.key_b, 8 * N}, {(void **)&tb.key2, 8 * N},
         {(void **)&tb.key3, 8 * N}, {(void **)&tb.idx_a, 4 * N}, {(void **)&tb.idx_b, 4 * N},
-        {(void **)&tb.sort_hist, 4 * 256 * sort_blocks}, {(void **)&tb.scan_tmp, 4 * scan_tiles},
+        {(void **)&tb.sort_scratch, sort_scratch_bytes(cap)}, {(void **)&tb.scan_tmp, 4 * scan_tiles},
         {(void **)&tb.body, 32 * N}, {(void **)&tb.onode, 32 * N},
         {(void **)&tb.bleft, 4 * N}, {(void **)&tb.bright, 4 * N}, {(void **)&tb.bparent, 4 * N},
         {(void **)&tb.leaf_bparent, 4 * N}, {(void **)&tb.bdelta, 4 * N},
@@ -210,6 +211,7 @@ int check_status(nbody_ctx *c) {
     if (h.status & kStatusCoincident)
         return fail(NBODY_ERR_COINCIDENT, "particles coincide to 63 octree levels (the reference recurses without bound)%s");
     if (h.status & kStatusCapacity) return fail(NBODY_ERR_CAPACITY, "walk stack spill capacity exceeded%s");
+    if (h.status & kStatusSortStall) return fail(NBODY_ERR_CUDA, "radix sort look-back gave up waiting%s");
     return NBODY_OK;
 }
 

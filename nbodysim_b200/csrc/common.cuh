@@ -29,7 +29,8 @@ enum : uint32_t {
     kStatusNonFinite = 1u << 0,
     kStatusCoincident = 1u << 1,
     kStatusCapacity = 1u << 2,
-    kStatusDeepGroup = 1u << 3,  // a group of equal 21-level keys needed deep keys
+    kStatusDeepGroup = 1u << 3,  // a group of equal 42-level keys needed a third key word
+    kStatusSortStall = 1u << 4,  // a radix-sort look-back gave up waiting (never expected)
 };
 
 struct DevScalars {

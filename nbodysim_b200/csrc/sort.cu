@@ -1,0 +1,190 @@
+// LSD radix sort of (u64 key, u32 index) pairs, one kernel per 8-bit pass.
+//
+// The global digit counts of every pass do not depend on the order of the
+// keys, so one kernel computes them for all passes up front. Each pass then
+// is a single kernel: a block takes the next tile (4096 keys) in ticket order,
+// ranks its keys stably (per warp, match_any over 16 rounds of 32 keys),
+// publishes its per-digit count, adds the counts of all earlier tiles by
+// decoupled look-back (a tile only ever waits for tiles that started before
+// it, so the wait always ends; it is still bounded, and a timeout is reported
+// as an error), and scatters.
+#include "sort.cuh"
+
+namespace nbody {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kItems = 16;
+constexpr uint32_t kTile = kThreads * kItems;
+constexpr uint32_t kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kValue = (1u << 30) - 1;
+constexpr uint32_t kSpinLimit = 1u << 20;
+
+// Global digit histograms of every pass. Pass p sorts by byte (p % 8) of word
+// p / 8, where the words are, in order, `w0` (8 passes), `w1` (8 passes) and
+// the 16-bit `w2` (2 passes, optional).
+__global__ void k_hist_all(const uint64_t *__restrict__ w0, const uint64_t *__restrict__ w1,
+                           const uint32_t *__restrict__ w2, uint32_t n, int npass, uint32_t *__restrict__ ghist) {
+    __shared__ uint32_t s_h[18 * 256];
+    for (int i = threadIdx.x; i < npass * 256; i += blockDim.x) s_h[i] = 0;
+    __syncthreads();
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint64_t a = w0[i], b = w1[i];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            atomicAdd(&s_h[k * 256 + ((a >> (8 * k)) & 255u)], 1u);
+            atomicAdd(&s_h[(8 + k) * 256 + ((b >> (8 * k)) & 255u)], 1u);
+        }
+        if (npass > 16) {
+            const uint32_t c = w2[i];
+            atomicAdd(&s_h[16 * 256 + (c & 255u)], 1u);
+            atomicAdd(&s_h[17 * 256 + ((c >> 8) & 255u)], 1u);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < npass * 256; i += blockDim.x)
+        if (s_h[i]) atomicAdd(&ghist[i], s_h[i]);
+}
+
+// Exclusive scan of each pass's 256 counts (one block per pass).
+__global__ void k_hist_scan(uint32_t *__restrict__ ghist) {
+    __shared__ uint32_t s[256];
+    uint32_t *h = ghist + 256 * blockIdx.x;
+    const int t = threadIdx.x;
+    const uint32_t x = h[t];
+    s[t] = x;
+    __syncthreads();
+    for (int o = 1; o < 256; o <<= 1) {
+        const uint32_t y = t >= o ? s[t - o] : 0u;
+        __syncthreads();
+        s[t] += y;
+        __syncthreads();
+    }
+    h[t] = s[t] - x;
+}
+
+__global__ void __launch_bounds__(kThreads) k_onesweep(const uint64_t *__restrict__ kin,
+                                                       const uint32_t *__restrict__ iin, uint64_t *__restrict__ kout,
+                                                       uint32_t *__restrict__ iout, uint32_t n, int shift,
+                                                       const uint32_t *__restrict__ goff, uint32_t *status,
+                                                       uint32_t *ticket, uint32_t *err, uint32_t err_bit) {
+    __shared__ uint32_t s_wc[kWarps][256];  // per-warp digit counts, then per-warp offsets
+    __shared__ uint32_t s_base[256];        // global position of the tile's first key of each digit
+    __shared__ uint32_t s_tile;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    if (t == 0) s_tile = atomicAdd(ticket, 1u);
+    for (int k = 0; k < kWarps; k++) s_wc[k][t] = 0;
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint32_t base = tile * kTile + (uint32_t)w * (32 * kItems);
+    const uint32_t lt = (1u << lane) - 1u;
+    uint64_t key[kItems];
+    uint32_t idx[kItems], rank[kItems];
+    // ---- load and rank: warp w owns keys [base, base + 512) in order
+#pragma unroll
+    for (int r = 0; r < kItems; r++) {
+        const uint32_t i = base + r * 32 + lane;
+        const bool valid = i < n;
+        key[r] = valid ? kin[i] : 0ull;
+        idx[r] = valid ? iin[i] : 0u;
+        const uint32_t d = (uint32_t)((key[r] >> shift) & 255u);
+        const uint32_t peers = __match_any_sync(0xffffffffu, valid ? d : 256u + lane);
+        const uint32_t before = valid ? s_wc[w][d] : 0u;
+        rank[r] = before + __popc(peers & lt);
+        __syncwarp();
+        if (valid && (peers & lt) == 0) s_wc[w][d] = before + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // ---- per digit (thread t = digit): offsets of each warp, tile total
+    uint32_t total = 0;
+#pragma unroll
+    for (int k = 0; k < kWarps; k++) {
+        const uint32_t c = s_wc[k][t];
+        s_wc[k][t] = total;
+        total += c;
+    }
+    // ---- decoupled look-back over earlier tiles
+    uint32_t *st = status + (size_t)tile * 256 + t;
+    uint32_t excl = 0;
+    if (tile == 0) {
+        atomicExch(st, kFlagInc | total);
+    } else {
+        atomicExch(st, kFlagAgg | total);
+        // read up to 8 predecessors per round trip, newest first
+        const volatile uint32_t *vs = status;
+        int64_t p = (int64_t)tile - 1;
+        uint32_t spins = 0;
+        bool done = false;
+        while (!done) {
+            uint32_t v[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) v[k] = p - k >= 0 ? vs[(size_t)(p - k) * 256 + t] : kFlagInc;
+            int used = 0;
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                if (done || used < k) continue;  // stop at the first entry not yet published
+                const uint32_t flag = v[k] & ~kValue;
+                if (flag == 0u) continue;
+                excl += v[k] & kValue;
+                used = k + 1;
+                if (flag == kFlagInc) done = true;
+            }
+            p -= used;
+            if (!done && used == 0 && ++spins > kSpinLimit) {
+                atomicOr(err, err_bit);
+                break;
+            }
+        }
+        __threadfence();
+        atomicExch(st, kFlagInc | (excl + total));
+    }
+    s_base[t] = goff[t] + excl;
+    __syncthreads();
+    // ---- scatter
+#pragma unroll
+    for (int r = 0; r < kItems; r++) {
+        const uint32_t i = base + r * 32 + lane;
+        if (i < n) {
+            const uint32_t d = (uint32_t)((key[r] >> shift) & 255u);
+            const uint32_t pos = s_base[d] + s_wc[w][d] + rank[r];
+            kout[pos] = key[r];
+            iout[pos] = idx[r];
+        }
+    }
+}
+
+}  // namespace
+
+size_t sort_scratch_bytes(uint32_t n) {
+    const size_t tiles = (n + kTile - 1) / kTile;
+    return 4 * (18 * 256 + 18 * tiles * 256 + 32);
+}
+
+cudaError_t sort_prepare(const uint64_t *w0, const uint64_t *w1, const uint32_t *w2, uint32_t n, int npass,
+                         uint32_t *scratch, cudaStream_t st, unsigned *launches) {
+    const size_t tiles = (n + kTile - 1) / kTile;
+    cudaError_t e = cudaMemsetAsync(scratch, 0, 4 * (18 * 256 + 18 * tiles * 256 + 32), st);
+    if (e != cudaSuccess) return e;
+    const unsigned blocks = (unsigned)std::min<size_t>(1184, (n + 255) / 256);
+    k_hist_all<<<blocks ? blocks : 1, 256, 0, st>>>(w0, w1, w2, n, npass, scratch);
+    k_hist_scan<<<npass, 256, 0, st>>>(scratch);
+    *launches += 2;
+    return cudaGetLastError();
+}
+
+cudaError_t sort_pass(const uint64_t *kin, const uint32_t *iin, uint64_t *kout, uint32_t *iout, uint32_t n, int pass,
+                      int shift, uint32_t *scratch, uint32_t *err, uint32_t err_bit, cudaStream_t st,
+                      unsigned *launches) {
+    const size_t tiles = (n + kTile - 1) / kTile;
+    uint32_t *goff = scratch + 256 * pass;
+    uint32_t *status = scratch + 18 * 256 + (size_t)pass * tiles * 256;
+    uint32_t *ticket = scratch + 18 * 256 + 18 * tiles * 256 + pass;
+    k_onesweep<<<(unsigned)tiles, kThreads, 0, st>>>(kin, iin, kout, iout, n, shift, goff, status, ticket, err,
+                                                     err_bit);
+    *launches += 1;
+    return cudaGetLastError();
+}
+
+}  // namespace nbody

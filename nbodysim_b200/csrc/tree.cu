@@ -8,6 +8,7 @@
 // emulated below, the same centre of mass as their bottom node, so every
 // particle's walk accepts the same bodies (see walk.cu).
 #include "tree.cuh"
+#include "sort.cuh"
 
 #include <cstdio>
 
@@ -188,27 +189,6 @@ __global__ void k_gather_sys(const uint32_t *__restrict__ sys_id, const uint32_t
     if (sys_sorted) sys_sorted[j] = s;
 }
 
-// ---------------------------------------------------------------------------
-// LSD radix sort of (key, idx), 8-bit digits, stable per pass:
-// histogram per tile -> exclusive scan (digit-major) -> ranked scatter.
-constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortThreads * kSortItems;
-
-__global__ void k_sort_hist(const uint64_t *__restrict__ key, uint32_t n, int shift,
-                            uint32_t *__restrict__ hist, uint32_t nblocks) {
-    __shared__ uint32_t s_h[256];
-    s_h[threadIdx.x] = 0;
-    __syncthreads();
-    uint32_t base = blockIdx.x * kSortTile;
-    for (int r = 0; r < kSortItems; r++) {
-        uint32_t i = base + r * kSortThreads + threadIdx.x;
-        if (i < n) atomicAdd(&s_h[(key[i] >> shift) & 255u], 1u);
-    }
-    __syncthreads();
-    hist[threadIdx.x * nblocks + blockIdx.x] = s_h[threadIdx.x];
-}
-
 // Exclusive prefix sum of u32 values in place: tiles of 4096 scanned per
 // block, tile totals scanned by one block, then added back.
 constexpr int kScanThreads = 1024;
@@ -283,50 +263,6 @@ unsigned scan_exclusive(uint32_t *v, uint32_t len, uint32_t *tile_sums, uint32_t
     k_scan_small<<<1, kScanThreads, 0, st>>>(tile_sums, tiles, total);
     if (tiles > 1) k_scan_add<<<(len + 255) / 256, 256, 0, st>>>(v, len, tile_sums);
     return tiles > 1 ? 3u : 2u;
-}
-
-__global__ void k_sort_scatter(const uint64_t *__restrict__ key_in, const uint32_t *__restrict__ idx_in,
-                               uint64_t *__restrict__ key_out, uint32_t *__restrict__ idx_out,
-                               uint32_t n, int shift, const uint32_t *__restrict__ hist,
-                               uint32_t nblocks) {
-    __shared__ uint32_t s_off[256];
-    __shared__ uint32_t s_w[kSortThreads / 32][256];
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    s_off[t] = hist[t * nblocks + blockIdx.x];
-    const uint32_t lt = (1u << lane) - 1u;
-    uint32_t base = blockIdx.x * kSortTile;
-    for (int r = 0; r < kSortItems; r++) {
-#pragma unroll
-        for (int w = 0; w < kSortThreads / 32; w++) s_w[w][t] = 0;
-        __syncthreads();
-        uint32_t i = base + r * kSortThreads + t;
-        bool valid = i < n;
-        uint64_t k = valid ? key_in[i] : 0;
-        uint32_t v = valid ? idx_in[i] : 0;
-        uint32_t d = (uint32_t)((k >> shift) & 255u);
-        uint32_t tag = valid ? d : (256u + lane);
-        uint32_t peers = __match_any_sync(0xffffffffu, tag);
-        uint32_t rank = __popc(peers & lt);
-        if (valid && rank == 0) s_w[warp][d] = __popc(peers);
-        __syncthreads();
-        {
-            uint32_t run = s_off[t];
-#pragma unroll
-            for (int w = 0; w < kSortThreads / 32; w++) {
-                uint32_t c = s_w[w][t];
-                s_w[w][t] = run;
-                run += c;
-            }
-            s_off[t] = run;
-        }
-        __syncthreads();
-        if (valid) {
-            uint32_t p = s_w[warp][d] + rank;
-            key_out[p] = k;
-            idx_out[p] = v;
-        }
-        __syncthreads();
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -559,10 +495,12 @@ __global__ void k_com(const double4 *__restrict__ body, const int32_t *__restric
         }
         const int32_t meta = ometa[p];
         const int nch = meta_nchild(meta);
-        __threadfence();
+        // Release: a thread that wrote a node (hops > 0) makes it visible
+        // before counting itself in; a leaf thread has written nothing.
+        if (hops > 0) __threadfence();
         uint32_t old = atomicAdd(&ocount[p], 1u);
         if (old != (uint32_t)(nch - 1)) return;
-        __threadfence();
+        __threadfence();  // acquire: the other children's results are visible
         const int L = meta_level(meta);
         double cm[8];
         double3 cc[8];
@@ -628,24 +566,25 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
     k_keys<<<blocks_for(n, 256), 256, 0, st>>>(tb.pos, n, tb.sc, tb.key3, tb.key_a, tb.key2, tb.idx_a,
                                                multi ? tb.sys_id : nullptr, tb.sys_root);
     L += 2;
-    // LSD radix sort by (k1, k2): 8 passes on k2, then 8 passes on k1.
-    const uint32_t nb = blocks_for(n, kSortTile);
-    auto passes = [&](uint64_t *kin, uint64_t *kout, uint32_t *iin, uint32_t *iout, int bits = 64) {
-        for (int shift = 0; shift < bits; shift += 8) {
-            k_sort_hist<<<nb, kSortThreads, 0, st>>>(kin, n, shift, tb.sort_hist, nb);
-            L += 2 + scan_exclusive(tb.sort_hist, 256u * nb, tb.scan_tmp, nullptr, st);
-            k_sort_scatter<<<nb, kSortThreads, 0, st>>>(kin, iin, kout, iout, n, shift, tb.sort_hist, nb);
+    // LSD radix sort by (system, k1, k2): 8 passes on k2, 8 on k1, 2 on the system id.
+    cudaError_t e = sort_prepare(tb.key2, tb.key3, multi ? tb.sys_id : nullptr, n, multi ? 18 : 16, tb.sort_scratch,
+                                 st, &L);
+    if (e != cudaSuccess) return e;
+    uint32_t *sort_err = &tb.sc->status;
+    auto passes = [&](uint64_t *kin, uint64_t *kout, uint32_t *iin, uint32_t *iout, int first, int count) {
+        for (int q = 0; q < count; q++) {
+            sort_pass(kin, iin, kout, iout, n, first + q, 8 * q, tb.sort_scratch, sort_err, kStatusSortStall, st, &L);
             uint64_t *tk = kin; kin = kout; kout = tk;
             uint32_t *ti = iin; iin = iout; iout = ti;
         }
     };
-    passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b);          // result: key_a, idx_a
+    passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b, 0, 8);    // result: key_a, idx_a
     k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key3, tb.idx_a, tb.key_b, n);  // k1 in that order
-    passes(tb.key_b, tb.key_a, tb.idx_a, tb.idx_b);          // result: key_b (k1 sorted), idx_a
+    passes(tb.key_b, tb.key_a, tb.idx_a, tb.idx_b, 8, 8);    // result: key_b (k1 sorted), idx_a
     if (multi) {
         // then by system (16-bit ids, 2 stable passes; result back in key_a / idx_a)
         k_gather_sys<<<blocks_for(n, 256), 256, 0, st>>>(tb.sys_id, tb.idx_a, tb.key_a, nullptr, n);
-        passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b, 16);
+        passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b, 16, 2);
         k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key3, tb.idx_a, tb.key_b, n);  // k1 sorted
         k_gather_sys<<<blocks_for(n, 256), 256, 0, st>>>(tb.sys_id, tb.idx_a, nullptr, tb.sys_sorted, n);
         L += 3;

@@ -15,7 +15,7 @@ struct TreeBuild {
     unsigned bbox_blocks;
     uint64_t *key_a, *key_b, *key2, *key3;
     uint32_t *idx_a, *idx_b;
-    uint32_t *sort_hist;        // 256 * ceil(n / 4096)
+    uint32_t *sort_scratch;     // sort_scratch_bytes(n)
     uint32_t *scan_tmp;         // ceil(max_len / 4096) + 1
     double4 *body;
     int32_t *bleft, *bright, *bparent, *leaf_bparent, *bdelta;
