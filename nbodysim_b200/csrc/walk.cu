@@ -36,6 +36,15 @@ constexpr float kTolRel = 32.0f * kU;
 constexpr float kTolPm = 20.0f * kU;
 constexpr float kTiny = 64.0f * kU;
 
+// 1/sqrt(x) in one special-function instruction (flush-to-zero; squared pair
+// distances are never subnormal), the same ~2 ulp accuracy as rsqrtf without
+// rsqrtf's subnormal fix-up instructions.
+__device__ inline float rsqrt_ftz(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 __device__ inline double exp2_neg(int L) {  // exactly 2^-L for 0 <= L <= 1022
     return __longlong_as_double((long long)(1023 - L) << 52);
 }
@@ -109,7 +118,7 @@ __device__ inline void spill_in(Sm &s, int &top, uint32_t &spill_top, const int2
 template <bool kDamp>
 __device__ inline float pair_f32(float dx, float dy, float dz, float gm, float &inv) {
     const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-    inv = rsqrtf(r2);
+    inv = rsqrt_ftz(r2);
     if constexpr (kDamp) {
         const float r = r2 * inv;
         return gm * inv / (r2 + expf(-r));
@@ -176,7 +185,7 @@ __device__ inline void force_near_f32(const double4 *nc, const uint32_t *nm, int
         const float dx = (float)(c.x - bx), dy = (float)(c.y - by), dz = (float)(c.z - bz);
         const float gm = (float)c.w;
         const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-        const float inv = rsqrtf(r2);
+        const float inv = rsqrt_ftz(r2);
         float f;
         if constexpr (kDamp) {
             const float r = r2 * inv;
@@ -199,7 +208,7 @@ template <bool kDamp, typename T>
 __device__ inline void pair_adjoint(T dx, T dy, T dz, T r2, T gm, T lax, T lay, T laz, T &vx, T &vy, T &vz,
                                     T &mterm) {
     T inv, g, h;
-    if constexpr (sizeof(T) == 4) inv = rsqrtf(r2);
+    if constexpr (sizeof(T) == 4) inv = rsqrt_ftz(r2);
     else inv = 1.0 / sqrt(r2);
     const T inv2 = inv * inv;
     if constexpr (kDamp) {
