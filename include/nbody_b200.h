@@ -206,6 +206,53 @@ typedef struct nbody_gen_params {
 void nbody_default_gen_params(nbody_gen_params *g);
 int nbody_generate(const nbody_gen_params *g, uint32_t n, double *pos, double *vel, double *mass);
 
+/* ---- frames and images -------------------------------------------------
+ * The reference's frame files and renderer, on host arrays or the resident state. */
+
+/* dir/NNNN.dat or dir/NNNN.txt (gen_filename, src/main.cpp:283-291; dir NULL: "./data"). */
+int nbody_frame_path(const char *dir, uint32_t frame, int binary, char *buf, size_t buflen);
+/* Binary frame (the resume format, src/main.cpp:730-743): per particle position, velocity,
+ * acceleration (3 each) and mass in the reference's datatype (datatype_bytes 8 or 4).
+ * acc may be NULL (written as zeros). */
+int nbody_write_dat(const char *path, uint32_t n, const double *pos, const double *vel, const double *acc,
+                    const double *mass, int datatype_bytes);
+/* Reads a binary frame; with pos == NULL only sets *n. acc may be NULL. */
+int nbody_read_dat(const char *path, int datatype_bytes, uint32_t *n, double *pos, double *vel, double *acc,
+                   double *mass);
+/* Text frame "x, y, z" per line, 6 significant digits (src/main.cpp:744-759). */
+int nbody_write_txt(const char *path, uint32_t n, const double *pos, int datatype_bytes);
+/* read_data's search (src/main.cpp:790-811): newest NNNN.dat <= num_frames in dir, or -1. */
+int nbody_find_resume_frame(const char *dir, uint32_t num_frames, int32_t *frame_out);
+
+/* The resident state as frame files dir/NNNN.dat (binary) and/or dir/NNNN.txt (text), the
+ * records dump writes after each frame's update (src/main.cpp:680-766). Accelerations are
+ * those of the last force pass (zeros before the first). */
+int nbody_save_frame(nbody_ctx *ctx, const char *dir, uint32_t frame, int binary, int text, int datatype_bytes);
+/* read_data (src/main.cpp:790-811): loads the newest dir/NNNN.dat <= num_frames into the
+ * resident state and sets *next_frame to that frame + 1, or to 0 (state untouched) when
+ * there is none. */
+int nbody_load_frame(nbody_ctx *ctx, const char *dir, uint32_t num_frames, int datatype_bytes,
+                     uint32_t *next_frame);
+
+typedef struct nbody_image_params {
+    uint32_t width, height; /* keys img_w, img_h */
+    int projection;         /* key projection: 0 front, 1 side, 2 top, 3 iso */
+    int color;              /* key color: 0 bw, 1 heat */
+    int adaptive;           /* key adaptive_brightness */
+    int nonlinear;          /* key nonlinear_brightness */
+    double scale;           /* key scale */
+    double brightness;      /* key brightness */
+} nbody_image_params;
+/* Defaults of set_default (src/main.cpp:1345-1352). */
+void nbody_default_image_params(nbody_image_params *p);
+/* write_image (src/main.cpp:556-678) on the GPU over the resident positions:
+ * the 24-bit bitmap the reference passes to FreeImage, rgb_out[(y*width + x)*3 +
+ * {R,G,B}], row y = 0 at the bottom of the image. With a fractional brightness the
+ * per-pixel sums may round in a different order than the reference's. */
+int nbody_render(nbody_ctx *ctx, const nbody_image_params *p, uint8_t *rgb_out);
+/* Binary PPM of such a bitmap, top row first. */
+int nbody_write_ppm(const char *path, uint32_t width, uint32_t height, const uint8_t *rgb);
+
 /* ---- errors ------------------------------------------------------------ */
 const char *nbody_status_string(int status);
 /* Thread-local text of the last failure (CUDA error string or argument check). */

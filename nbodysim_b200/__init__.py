@@ -91,6 +91,11 @@ class Diagnostics(C.Structure):
                     mass=self.mass, com=tuple(self.com))
 
 
+class ImageParams(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("projection", C.c_int), ("color", C.c_int),
+                ("adaptive", C.c_int), ("nonlinear", C.c_int), ("scale", C.c_double), ("brightness", C.c_double)]
+
+
 class DeviceView(C.Structure):
     _fields_ = [("n", C.c_uint32), ("pos", C.c_void_p), ("vel", C.c_void_p), ("mass", C.c_void_p),
                 ("acc", C.c_void_p), ("acc_is_double", C.c_int)]
@@ -125,6 +130,17 @@ _SIGS = {
                                   C.c_void_p]),
     "nbody_forward_checkpointed": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32]),
     "nbody_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "nbody_frame_path": (C.c_int, [C.c_char_p, C.c_uint32, C.c_int, C.c_char_p, C.c_size_t]),
+    "nbody_write_dat": (C.c_int, [C.c_char_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "nbody_read_dat": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_void_p]),
+    "nbody_write_txt": (C.c_int, [C.c_char_p, C.c_uint32, C.c_void_p, C.c_int]),
+    "nbody_find_resume_frame": (C.c_int, [C.c_char_p, C.c_uint32, C.POINTER(C.c_int32)]),
+    "nbody_save_frame": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint32, C.c_int, C.c_int, C.c_int]),
+    "nbody_load_frame": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint32, C.c_int, C.POINTER(C.c_uint32)]),
+    "nbody_default_image_params": (None, [C.POINTER(ImageParams)]),
+    "nbody_render": (C.c_int, [C.c_void_p, C.POINTER(ImageParams), C.c_void_p]),
+    "nbody_write_ppm": (C.c_int, [C.c_char_p, C.c_uint32, C.c_uint32, C.c_void_p]),
     "nbody_probe_fp32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "nbody_root_cube_noalloc_max_n": (C.c_uint32, []),
     "nbody_root_cube_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
@@ -335,6 +351,25 @@ class Engine:
                                         m0.ctypes.data))
         return p0, v0, m0
 
+    def save_frame(self, dir: str, frame: int, binary: bool = True, text: bool = False,
+                   datatype_bytes: int = 8) -> None:
+        _check(self._lib.nbody_save_frame(self._h, dir.encode(), frame, int(binary), int(text), datatype_bytes))
+
+    def load_frame(self, dir: str, num_frames: int, datatype_bytes: int = 8) -> int:
+        """Resumes from the newest binary frame <= num_frames; returns the next frame (0: none found)."""
+        nxt = C.c_uint32(0)
+        _check(self._lib.nbody_load_frame(self._h, dir.encode(), num_frames, datatype_bytes, C.byref(nxt)))
+        if nxt.value:
+            self.n = self.device_view().n
+        return nxt.value
+
+    def render(self, params: ImageParams | None = None, **kw):
+        """The reference's write_image on the resident positions: (height, width, 3) uint8, [y, x]."""
+        p = params if params is not None else image_params(**kw)
+        out = np.zeros((p.height, p.width, 3), np.uint8)
+        _check(self._lib.nbody_render(self._h, C.byref(p), out.ctypes.data))
+        return out
+
     def stats(self) -> dict:
         s = Stats()
         _check(self._lib.nbody_get_stats(self._h, C.byref(s)))
@@ -349,6 +384,56 @@ class Engine:
         v = DeviceView()
         _check(self._lib.nbody_device_view_get(self._h, C.byref(v)))
         return v
+
+
+def frame_path(dir: str | None, frame: int, binary: bool) -> str:
+    buf = C.create_string_buffer(4096)
+    _check(load_library().nbody_frame_path(dir.encode() if dir else None, frame, int(binary), buf, 4096))
+    return buf.value.decode()
+
+
+def write_dat(path: str, pos, vel, mass, acc=None, datatype_bytes: int = 8) -> None:
+    """The reference's binary frame (resume) format."""
+    pos = _aos(pos); n = pos.shape[0]; vel = _aos(vel, n); mass = _vec(mass, n)
+    acc = _aos(acc, n) if acc is not None else None
+    _check(load_library().nbody_write_dat(path.encode(), n, pos.ctypes.data, vel.ctypes.data, _ptr(acc),
+                                          mass.ctypes.data, datatype_bytes))
+
+
+def read_dat(path: str, datatype_bytes: int = 8):
+    """(pos, vel, acc, mass) of a binary frame, in file order."""
+    lib = load_library()
+    n = C.c_uint32(0)
+    _check(lib.nbody_read_dat(path.encode(), datatype_bytes, C.byref(n), None, None, None, None))
+    pos = np.zeros((n.value, 3)); vel = np.zeros((n.value, 3)); acc = np.zeros((n.value, 3)); mass = np.zeros(n.value)
+    _check(lib.nbody_read_dat(path.encode(), datatype_bytes, C.byref(n), pos.ctypes.data, vel.ctypes.data,
+                              acc.ctypes.data, mass.ctypes.data))
+    return pos, vel, acc, mass
+
+
+def write_txt(path: str, pos, datatype_bytes: int = 8) -> None:
+    pos = _aos(pos)
+    _check(load_library().nbody_write_txt(path.encode(), pos.shape[0], pos.ctypes.data, datatype_bytes))
+
+
+def find_resume_frame(dir: str, num_frames: int) -> int:
+    f = C.c_int32(0)
+    _check(load_library().nbody_find_resume_frame(dir.encode(), num_frames, C.byref(f)))
+    return f.value
+
+
+def image_params(**kw) -> ImageParams:
+    p = ImageParams()
+    load_library().nbody_default_image_params(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def write_ppm(path: str, rgb) -> None:
+    rgb = np.ascontiguousarray(rgb, dtype=np.uint8)
+    h, w, _ = rgb.shape
+    _check(load_library().nbody_write_ppm(path.encode(), w, h, rgb.ctypes.data))
 
 
 def probe_fp32_peak(device: int = 0) -> tuple[float, float]:

@@ -22,6 +22,7 @@
 #include "tree.cuh"
 #include "sort.cuh"
 #include "walk.cuh"
+#include "image.cuh"
 
 using namespace nbody;
 
@@ -102,6 +103,9 @@ struct nbody_ctx {
     unsigned step_launches = 0;
     std::vector<cudaGraphExec_t> rec_exec, adj_exec;
     std::vector<unsigned> rec_launches, adj_launches;
+    // image rendering buffers (grown on demand)
+    void *img_arena = nullptr;
+    size_t img_bytes = 0;
 };
 
 namespace {
@@ -640,6 +644,7 @@ int nbody_destroy(nbody_ctx *c) {
     if (c->arena) cudaFree(c->arena);
     if (c->adj_arena) cudaFree(c->adj_arena);
     if (c->sys_arena) cudaFree(c->sys_arena);
+    if (c->img_arena) cudaFree(c->img_arena);
     if (c->sc) cudaFree(c->sc);
     if (c->hsc) cudaFreeHost(c->hsc);
     for (auto &e : c->ev)
@@ -1012,6 +1017,98 @@ int nbody_backward(nbody_ctx *c, const double *dL_dpos, const double *dL_dvel, d
     NB_CUDA(cudaMemcpyAsync(dL_dmass, c->lm, 8 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
     if ((rc = copy_scalars_back(c))) return rc;
     return check_status(c);
+}
+
+int nbody_save_frame(nbody_ctx *c, const char *dir, uint32_t frame, int binary, int text, int datatype_bytes) {
+    CTX_OR_FAIL(c);
+    if (!c->have_state) return fail(NBODY_ERR_STATE, "no particles set%s");
+    if (datatype_bytes != 8 && datatype_bytes != 4) return fail(NBODY_ERR_INVALID, "datatype_bytes must be 8 or 4%s");
+    const size_t n = c->n;
+    std::vector<double> pos(3 * n), vel(3 * n, 0.0), acc(3 * n, 0.0), mass(n);
+    int rc = nbody_get_particles(c, pos.data(), c->have_vel ? vel.data() : nullptr, c->have_acc ? acc.data() : nullptr);
+    if (rc) return rc;
+    NB_CUDA(cudaMemcpyAsync(mass.data(), c->mass, 8 * n, cudaMemcpyDeviceToHost, c->stream));
+    NB_CUDA(cudaStreamSynchronize(c->stream));
+    char path[4096];
+    if (binary) {
+        if (nbody_frame_path(dir, frame, 1, path, sizeof path) ||
+            nbody_write_dat(path, c->n, pos.data(), vel.data(), acc.data(), mass.data(), datatype_bytes))
+            return fail(NBODY_ERR_INVALID, "cannot write binary frame %s", path);
+    }
+    if (text) {
+        if (nbody_frame_path(dir, frame, 0, path, sizeof path) ||
+            nbody_write_txt(path, c->n, pos.data(), datatype_bytes))
+            return fail(NBODY_ERR_INVALID, "cannot write text frame %s", path);
+    }
+    return NBODY_OK;
+}
+
+int nbody_load_frame(nbody_ctx *c, const char *dir, uint32_t num_frames, int datatype_bytes, uint32_t *next_frame) {
+    CTX_OR_FAIL(c);
+    if (!next_frame) return fail(NBODY_ERR_INVALID, "next_frame is null%s");
+    int32_t f = -1;
+    if (nbody_find_resume_frame(dir, num_frames, &f)) return fail(NBODY_ERR_INVALID, "bad frame directory%s");
+    if (f < 0) {  // nothing to resume: read_data returns 0 and the caller generates
+        *next_frame = 0;
+        return NBODY_OK;
+    }
+    char path[4096];
+    uint32_t n = 0;
+    if (nbody_frame_path(dir, (uint32_t)f, 1, path, sizeof path) ||
+        nbody_read_dat(path, datatype_bytes, &n, nullptr, nullptr, nullptr, nullptr))
+        return fail(NBODY_ERR_INVALID, "cannot read %s", path);
+    std::vector<double> pos(3 * (size_t)n), vel(3 * (size_t)n), mass(n);
+    if (nbody_read_dat(path, datatype_bytes, &n, pos.data(), vel.data(), nullptr, mass.data()))
+        return fail(NBODY_ERR_INVALID, "cannot read %s", path);
+    int rc = nbody_set_particles(c, n, pos.data(), vel.data(), mass.data());
+    if (rc) return rc;
+    *next_frame = (uint32_t)f + 1;
+    return NBODY_OK;
+}
+
+void nbody_default_image_params(nbody_image_params *p) {
+    if (!p) return;
+    p->width = 1920;        // img_w, src/main.cpp:1347
+    p->height = 1080;       // img_h, src/main.cpp:1348
+    p->projection = 3;      // iso, src/main.cpp:1346
+    p->color = 0;           // bw, src/main.cpp:1350
+    p->adaptive = 0;        // adaptive_brightness, src/main.cpp:1351
+    p->nonlinear = 0;       // nonlinear_brightness, src/main.cpp:1352
+    p->scale = 1.0;         // scale, src/main.cpp:1349
+    p->brightness = 255.0;  // brightness, src/main.cpp:1345
+}
+
+int nbody_render(nbody_ctx *c, const nbody_image_params *ip, uint8_t *rgb_out) {
+    CTX_OR_FAIL(c);
+    if (!ip || !rgb_out || ip->width == 0 || ip->height == 0 || ip->projection < 0 || ip->projection > 3 ||
+        ip->color < 0 || ip->color > 1 || (uint64_t)ip->width * ip->height > (1ull << 28))
+        return fail(NBODY_ERR_INVALID, "invalid image parameters%s");
+    if (!c->have_state) return fail(NBODY_ERR_STATE, "no particles set%s");
+    const size_t pixels = (size_t)ip->width * ip->height;
+    const size_t need = align256(8 * pixels) + align256(8) + align256(3 * pixels);
+    if (need > c->img_bytes) {
+        NB_CUDA(cudaStreamSynchronize(c->stream));
+        if (c->img_arena) NB_CUDA(cudaFree(c->img_arena));
+        c->img_arena = nullptr;
+        c->img_bytes = 0;
+        cudaError_t e = cudaMalloc(&c->img_arena, need);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(NBODY_ERR_OOM, "image buffers (%s)", cudaGetErrorString(e));
+        }
+        c->img_bytes = need;
+    }
+    char *p = (char *)c->img_arena;
+    double *grid = (double *)p;
+    unsigned long long *maxbits = (unsigned long long *)(p + align256(8 * pixels));
+    uint8_t *rgb = (uint8_t *)(p + align256(8 * pixels) + align256(8));
+    ImageArgs a{ip->width, ip->height, ip->projection, ip->color, ip->adaptive, ip->nonlinear, ip->scale,
+                ip->brightness};
+    NB_CUDA(render_image(c->pos, c->n, a, grid, maxbits, rgb, c->stream));
+    c->launches += 3;
+    NB_CUDA(cudaMemcpyAsync(rgb_out, rgb, 3 * pixels, cudaMemcpyDeviceToHost, c->stream));
+    NB_CUDA(cudaStreamSynchronize(c->stream));
+    return NBODY_OK;
 }
 
 const char *nbody_status_string(int s) {

@@ -102,6 +102,8 @@ class Reference:
         L.ref_tree_nodes.argtypes = [C.c_uint, C.c_void_p, C.c_void_p, C.c_uint, C.c_int,
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.c_void_p]
+        L.ref_write_image.argtypes = [C.c_uint, C.c_void_p, C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_int, C.c_int,
+                                      C.c_double, C.c_double, C.c_void_p]
         self.datatype_bytes = L.ref_datatype_bytes()
 
     def generate(self, g: GenParams, n: int):
@@ -131,6 +133,17 @@ class Reference:
         self.lib.ref_run_frames(n, pos.ctypes.data, vel.ctypes.data, mass.ctypes.data, theta, int(damping),
                                 dt, threads, frames, out.ctypes.data if out is not None else None)
         return pos, vel, out
+
+    def write_image(self, pos, width=1920, height=1080, projection=3, color=0, adaptive=False, nonlinear=False,
+                    scale=1.0, brightness=255.0):
+        """The reference's write_image; returns an (height, width, 3) uint8 array indexed [y, x]."""
+        pos = _c64(pos)
+        out = np.zeros((height, width, 3), np.uint8)
+        rc = self.lib.ref_write_image(len(pos), pos.ctypes.data, width, height, projection, color, int(adaptive),
+                                      int(nonlinear), scale, brightness, out.ctypes.data)
+        if rc:
+            raise RuntimeError("reference write_image failed")
+        return out
 
     def tree_nodes(self, pos, mass, threads=1):
         pos = _c64(pos); mass = _c64(mass); n = len(mass)

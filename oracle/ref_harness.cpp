@@ -255,6 +255,26 @@ int ref_run_frames(unsigned int n, double *pos, double *vel, const double *mass,
     return 0;
 }
 
+/* The reference's write_image (src/main.cpp:556-678) on n positions; the
+ * rendered 24-bit bitmap comes back through the FreeImage stand-in:
+ * rgb_out[(y * w + x) * 3 + {R, G, B}], y as FreeImage counts it (row 0 at the
+ * bottom of the saved image). Returns 0 on success. */
+int ref_write_image(unsigned int n, const double *pos, unsigned int img_w, unsigned int img_h,
+                    unsigned int projection, unsigned int color, int adaptive, int nonlinear, double scale,
+                    double brightness, unsigned char *rgb_out) {
+    std::vector<particle *> order;
+    particle_set set;
+    std::vector<double> mass(n, 1.0);
+    make_particles(n, pos, NULL, mass.data(), order, set);
+    g_stub_last_image = FIBITMAP{0, 0, std::vector<unsigned char>()};
+    write_image(img_w, img_h, projection, color, adaptive != 0, nonlinear != 0, (datatype)scale,
+                (datatype)brightness, 0, &set);
+    free_particles(order);
+    if (g_stub_last_image.w != (int)img_w || g_stub_last_image.h != (int)img_h) return -1;
+    std::memcpy(rgb_out, g_stub_last_image.rgb.data(), g_stub_last_image.rgb.size());
+    return 0;
+}
+
 /* The reference's unmodified main() (src/main.cpp:1359-1504), for running the
  * whole program in-process: argv[1] is a settings file; output goes to ./data. */
 int ref_main(int argc, char **argv) { return nbodysim_reference_main(argc, argv); }

@@ -91,3 +91,18 @@ def test_oracle_frames_equal_reference_live(orc, ref, oracle_mod):
     _, _, f1 = ref.run_frames(p, v, m, 4, keep_frames=True)
     _, _, f2 = orc.run_frames(p, v, m, 4, keep_frames=True)
     assert np.array_equal(f1, f2)
+
+
+def test_reference_image_hand_cases(ref):
+    """write_image (src/main.cpp:556-678) on single particles, worked by hand."""
+    import numpy as np
+    # front: x = px + w/2 = 5, y = pz + h/2 = 1
+    im = ref.write_image(np.array([[1.0, 0.0, -2.0]]), 8, 6, 0, 0, False, False, 1.0, 255.0)
+    assert im[1, 5].tolist() == [255, 255, 255] and im.sum() == 3 * 255
+    # iso at the origin: x = w/2 = 4, y = h/2 = 3, flipped to h-1-3 = 2; heat 300 -> (R, G, B) = (44, 211, 0)
+    im = ref.write_image(np.array([[0.0, 0.0, 0.0]]), 8, 6, 3, 1, False, False, 1.0, 300.0)
+    assert im[2, 4].tolist() == [44, 211, 0]
+    assert (im[:, :, 2] == 255).sum() == 8 * 6 - 1  # every other pixel is heat 0: blue
+    # y between h-1 and w-1 is clamped onto the top row (the bound uses the width)
+    im = ref.write_image(np.array([[0.0, 0.0, 4.0]]), 12, 6, 0, 0, False, False, 1.0, 10.0)
+    assert im[5, 6].tolist() == [10, 10, 10]
