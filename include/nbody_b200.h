@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define NBODY_ABI_VERSION 2  /* 2: nbody_params.autotune, nbody_stats walk fields */
+#define NBODY_ABI_VERSION 3  /* 2: nbody_params.autotune, nbody_stats walk fields; 3: merging */
 
 /* ---- status codes ---------------------------------------------------- */
 #define NBODY_OK 0
@@ -67,6 +67,15 @@ typedef struct nbody_params {
     int precision;          /* NBODY_PRECISION_* */
     int device;             /* CUDA device ordinal */
     int autotune;           /* run nbody_autotune on the first step at each new size (default 0) */
+    /* Merging, applied by nbody_step only (single system; not with the adjoint or
+     * nbody_step_host, which keep n fixed). Each step may then shrink n; read it back
+     * with nbody_device_view_get. */
+    int collide;            /* key `collide` (src/main.cpp:130): merge particles closer than
+                               collision_range that the walk accepts as leaves (src/main.cpp:386-396) */
+    double collision_range; /* key `collision_range` (src/main.cpp:153, default 0.01) */
+    double min_node_size;   /* key `min_node_size` (src/main.cpp:159): > 0 merges every cell
+                               smaller than this into one particle before the forces
+                               (apply_minimum_size, src/main.cpp:1001-1060) */
 } nbody_params;
 
 /* Defaults of the reference's set_default (src/main.cpp:1312-1357) for the keys above;
@@ -105,6 +114,8 @@ int nbody_set_particles(nbody_ctx *ctx, uint32_t n, const double *pos, const dou
 int nbody_set_systems(nbody_ctx *ctx, uint32_t nsys, const uint32_t *counts);
 /* Any output pointer may be NULL. acc is the last computed acceleration. */
 int nbody_get_particles(nbody_ctx *ctx, double *pos, double *vel, double *acc);
+/* Masses of the resident state (they change only by merging). */
+int nbody_get_masses(nbody_ctx *ctx, double *mass);
 /* nsteps full steps: root cube -> octree -> mass/COM -> walk+force -> (adaptive dt) -> update. */
 int nbody_step(nbody_ctx *ctx, uint32_t nsteps);
 /* Forces only, on the resident state (acc stays on the device). */
@@ -144,6 +155,9 @@ typedef struct nbody_stats {
     double root_center[3];
     double root_side;
     float ms_tree, ms_com, ms_walk, ms_update; /* last pass, CUDA events; 0 if not timed */
+    uint64_t merged_min_size;  /* particles removed by minimum-size merges in the last nbody_step */
+    uint64_t merged_collisions; /* particles removed by collision merges in the last nbody_step */
+    uint64_t collision_pairs;  /* (particle, leaf) pairs found within range, last nbody_step */
 } nbody_stats;
 int nbody_get_stats(nbody_ctx *ctx, nbody_stats *out);
 /* Time phases with CUDA events on the context stream (default off; timed calls

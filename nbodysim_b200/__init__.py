@@ -48,6 +48,7 @@ class Params(C.Structure):
         ("theta", C.c_double), ("dt", C.c_double), ("damping", C.c_int), ("adaptive", C.c_int),
         ("min_adaptive_dt", C.c_double), ("max_pos_change", C.c_double), ("max_vel_change", C.c_double),
         ("precision", C.c_int), ("device", C.c_int), ("autotune", C.c_int),
+        ("collide", C.c_int), ("collision_range", C.c_double), ("min_node_size", C.c_double),
     ]
 
 
@@ -71,6 +72,7 @@ class Stats(C.Structure):
         ("max_stack", C.c_uint32), ("fallback_tests", C.c_uint32), ("last_dt", C.c_double),
         ("root_center", C.c_double * 3), ("root_side", C.c_double),
         ("ms_tree", C.c_float), ("ms_com", C.c_float), ("ms_walk", C.c_float), ("ms_update", C.c_float),
+        ("merged_min_size", C.c_uint64), ("merged_collisions", C.c_uint64), ("collision_pairs", C.c_uint64),
     ]
 
     def as_dict(self) -> dict:
@@ -136,6 +138,7 @@ _SIGS = {
                                  C.c_void_p]),
     "nbody_write_txt": (C.c_int, [C.c_char_p, C.c_uint32, C.c_void_p, C.c_int]),
     "nbody_find_resume_frame": (C.c_int, [C.c_char_p, C.c_uint32, C.POINTER(C.c_int32)]),
+    "nbody_get_masses": (C.c_int, [C.c_void_p, C.c_void_p]),
     "nbody_save_frame": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint32, C.c_int, C.c_int, C.c_int]),
     "nbody_load_frame": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint32, C.c_int, C.POINTER(C.c_uint32)]),
     "nbody_default_image_params": (None, [C.POINTER(ImageParams)]),
@@ -202,10 +205,13 @@ def default_params(**kw) -> Params:
 
 
 def params_from_settings(s: Settings, **kw) -> Params:
-    """Engine parameters from the reference's config keys."""
+    """Engine parameters from the reference's config keys. As in the reference's
+    frame loop (src/main.cpp:1425), min_node_size only takes effect with verbose."""
     return default_params(theta=s.theta, dt=s.dt, damping=int(s.damping), adaptive=int(s.adaptive),
                           min_adaptive_dt=s.min_adaptive_dt, max_pos_change=s.max_pos_change,
-                          max_vel_change=s.max_vel_change, **kw)
+                          max_vel_change=s.max_vel_change, collide=int(s.collide),
+                          collision_range=s.collision_range,
+                          min_node_size=s.min_node_size if s.verbose else 0.0, **kw)
 
 
 def gen_params(**kw) -> GenParams:
@@ -313,6 +319,13 @@ class Engine:
 
     def step(self, nsteps: int = 1) -> None:
         _check(self._lib.nbody_step(self._h, nsteps))
+        if self.n and (self.params.collide or self.params.min_node_size > 0):
+            self.n = self.device_view().n  # merging may have removed particles
+
+    def get_masses(self):
+        m = np.zeros(self.n)
+        _check(self._lib.nbody_get_masses(self._h, m.ctypes.data))
+        return m
 
     def compute_forces(self) -> None:
         _check(self._lib.nbody_compute_forces(self._h))

@@ -23,6 +23,7 @@
 #include "sort.cuh"
 #include "walk.cuh"
 #include "image.cuh"
+#include "merge.cuh"
 
 using namespace nbody;
 
@@ -106,6 +107,14 @@ struct nbody_ctx {
     // image rendering buffers (grown on demand)
     void *img_arena = nullptr;
     size_t img_bytes = 0;
+    // merging (collisions, minimum node size): buffers sized for cap, pairs grown on demand
+    void *merge_arena = nullptr;
+    size_t merge_bytes = 0;
+    uint32_t merge_cap = 0;
+    MergeBufs mb{};
+    uint2 *pairs = nullptr;
+    uint32_t *hcounters = nullptr;  // pinned mirror of mb.counters
+    uint64_t merged_min_size = 0, merged_collisions = 0, collision_pairs = 0;
 };
 
 namespace {
@@ -123,6 +132,10 @@ int check_params(const nbody_params *p) {
         return fail(NBODY_ERR_INVALID, "unknown precision%s");
     if (p->adaptive && (!(p->max_pos_change > 0) || !(p->max_vel_change > 0) || !(p->min_adaptive_dt >= 0)))
         return fail(NBODY_ERR_INVALID, "adaptive dt needs max_pos_change > 0, max_vel_change > 0, min_adaptive_dt >= 0%s");
+    if (!(p->collision_range >= 0) || !std::isfinite(p->collision_range))
+        return fail(NBODY_ERR_INVALID, "collision_range must be finite and >= 0%s");
+    if (!(p->min_node_size >= 0) || !std::isfinite(p->min_node_size))
+        return fail(NBODY_ERR_INVALID, "min_node_size must be finite and >= 0%s");
     return NBODY_OK;
 }
 
@@ -198,6 +211,9 @@ int check_status(nbody_ctx *c) {
         s.walk_warps_per_block = w.warps;
         s.walk_blocks = w.blocks;
     }
+    s.merged_min_size = c->merged_min_size;
+    s.merged_collisions = c->merged_collisions;
+    s.collision_pairs = c->collision_pairs;
     s.tree_nodes = h.n_onodes;
     s.tree_depth = h.depth;
     s.max_stack = h.max_stack;
@@ -233,10 +249,12 @@ void ev(nbody_ctx *c, int k) {
 }
 
 // One force pass on the resident pos/mass: tree, COM, walk. Asynchronous.
+int apply_min_size(nbody_ctx *c, bool want_vmax, unsigned *launches);
+
 int force_pass(nbody_ctx *c, int damping, double theta, bool fp64, bool want_vmax, bool track_amax,
                bool want_counts, bool want_pot, const double *pos = nullptr, bool adjoint = false,
-               const WalkLaunch *shape = nullptr) {
-    const uint32_t n = c->n;
+               const WalkLaunch *shape = nullptr, bool min_size = false) {
+    uint32_t n = c->n;
     unsigned launches = 1;
     NB_CUDA(launch_reset_pass(c->sc, c->stream));
     tree_inputs(c, n, want_vmax);
@@ -250,6 +268,11 @@ int force_pass(nbody_ctx *c, int damping, double theta, bool fp64, bool want_vma
     c->tb.sys_root_node = c->sys_root_node;
     ev(c, 0);
     NB_CUDA(build_octree(c->tb, c->stream, &launches));
+    if (min_size && c->p.min_node_size > 0 && n >= 2 && !multi) {
+        int rc = apply_min_size(c, want_vmax, &launches);
+        if (rc) return rc;
+        n = c->n;
+    }
     ev(c, 1);
     NB_CUDA(compute_com(c->tb, c->stream, &launches));
     ev(c, 2);
@@ -390,18 +413,183 @@ bool capture(nbody_ctx *c, cudaGraphExec_t *out, unsigned *launches, F &&body) {
     return ok;
 }
 
+// ---- merging ------------------------------------------------------------------
+bool merging(const nbody_ctx *c) { return c->p.collide || c->p.min_node_size > 0; }
+
+int reserve_merge(nbody_ctx *c) {
+    if (c->merge_arena && c->merge_cap >= c->cap) return NBODY_OK;
+    const size_t N = c->cap;
+    MergeBufs &m = c->mb;
+    struct Piece { void **dst; size_t bytes; };
+    Piece pieces[] = {
+        {(void **)&m.label, 4 * N}, {(void **)&m.rep, 4 * N}, {(void **)&m.flag, 4 * N}, {(void **)&m.offs, 4 * N},
+        {(void **)&m.scan_tmp, 4 * ((N + 4095) / 4096 + 8)},
+        {(void **)&m.mpos, 24 * N}, {(void **)&m.mvel, 24 * N}, {(void **)&m.mmass, 8 * N},
+        {(void **)&m.pos2, 24 * N}, {(void **)&m.vel2, 24 * N}, {(void **)&m.mass2, 8 * N}, {(void **)&m.acc2, 24 * N},
+        {(void **)&m.skey_a, 8 * N}, {(void **)&m.skey_b, 8 * N}, {(void **)&m.sidx_a, 4 * N},
+        {(void **)&m.sidx_b, 4 * N}, {(void **)&m.sort_scratch, sort_scratch_bytes(c->cap)},
+        {(void **)&m.counters, 4 * kMcCount},
+    };
+    size_t total = 0;
+    for (auto &pc : pieces) total += align256(pc.bytes);
+    NB_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->merge_arena) NB_CUDA(cudaFree(c->merge_arena));
+    c->merge_arena = nullptr;
+    c->merge_cap = 0;
+    cudaError_t e = cudaMalloc(&c->merge_arena, total);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        c->merge_arena = nullptr;
+        return fail(NBODY_ERR_OOM, "merge buffers (%s)", cudaGetErrorString(e));
+    }
+    char *p = (char *)c->merge_arena;
+    for (auto &pc : pieces) {
+        *pc.dst = p;
+        p += align256(pc.bytes);
+    }
+    c->merge_bytes = total;
+    c->merge_cap = c->cap;
+    if (!c->hcounters) {
+        if (cudaMallocHost(&c->hcounters, 4 * kMcCount) != cudaSuccess) {
+            cudaGetLastError();
+            c->hcounters = nullptr;
+            return fail(NBODY_ERR_OOM, "pinned counters%s");
+        }
+    }
+    return NBODY_OK;
+}
+
+int reserve_pairs(nbody_ctx *c, uint32_t need) {
+    if (c->pairs && c->mb.pair_cap >= need) return NBODY_OK;
+    uint32_t cap = std::max<uint32_t>(need + need / 2, 4096u);
+    NB_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->pairs) NB_CUDA(cudaFree(c->pairs));
+    c->pairs = nullptr;
+    c->mb.pair_cap = 0;
+    cudaError_t e = cudaMalloc(&c->pairs, sizeof(uint2) * (size_t)cap);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        c->pairs = nullptr;
+        return fail(NBODY_ERR_OOM, "collision pair buffer (%s)", cudaGetErrorString(e));
+    }
+    c->mb.pairs = c->pairs;
+    c->mb.pair_cap = cap;
+    return NBODY_OK;
+}
+
+// Waits for the stream and reads the merge counters; fails on a merge status bit.
+int read_counters(nbody_ctx *c) {
+    NB_CUDA(cudaMemcpyAsync(c->hcounters, c->mb.counters, 4 * kMcCount, cudaMemcpyDeviceToHost, c->stream));
+    NB_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->hcounters[kMcStatus])
+        return fail(NBODY_ERR_CUDA, "particle merging failed (status bits %s)",
+                    c->hcounters[kMcStatus] & kMergeStatusSort ? "sort" : "tree/union");
+    return NBODY_OK;
+}
+
+Tree tree_view(nbody_ctx *c) {
+    Tree t{};
+    t.n = c->n;
+    t.body = c->tb.body;
+    t.sidx = c->tb.idx_a;
+    t.onode = c->tb.onode;
+    t.ochild = c->tb.ochild;
+    t.ometa = c->tb.ometa;
+    t.sc = c->sc;
+    return t;
+}
+
+// Compacts to the kept particles (merged values at the representatives) and
+// adopts the new count; returns the number removed.
+int adopt_compaction(nbody_ctx *c, bool fp64, unsigned *launches, uint64_t *removed) {
+    const uint32_t n = c->n;
+    NB_CUDA(merge_compact(c->mb, n, c->pos, c->vel, c->mass, c->acc, fp64, c->stream, launches));
+    int rc = read_counters(c);
+    if (rc) return rc;
+    const uint32_t kept = c->hcounters[kMcKept];
+    if (kept == 0 || kept > n) return fail(NBODY_ERR_CUDA, "particle merging kept an impossible count%s");
+    NB_CUDA(cudaMemcpyAsync(c->pos, c->mb.pos2, 24 * (size_t)kept, cudaMemcpyDeviceToDevice, c->stream));
+    NB_CUDA(cudaMemcpyAsync(c->vel, c->mb.vel2, 24 * (size_t)kept, cudaMemcpyDeviceToDevice, c->stream));
+    NB_CUDA(cudaMemcpyAsync(c->mass, c->mb.mass2, 8 * (size_t)kept, cudaMemcpyDeviceToDevice, c->stream));
+    NB_CUDA(cudaMemcpyAsync(c->acc, c->mb.acc2, (fp64 ? 24 : 12) * (size_t)kept, cudaMemcpyDeviceToDevice,
+                            c->stream));
+    *removed = n - kept;
+    c->n = kept;
+    c->have_fwd = false;
+    return NBODY_OK;
+}
+
+// apply_minimum_size on the octree just built; rebuilds it in the same root
+// cube when anything merged (the reference keeps its root).
+int apply_min_size(nbody_ctx *c, bool want_vmax, unsigned *launches) {
+    int rc = reserve_merge(c);
+    if (rc) return rc;
+    const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
+    NB_CUDA(merge_begin(c->mb, c->n, c->stream, launches));
+    NB_CUDA(merge_min_size(c->mb, tree_view(c), c->tb.oparent, c->vel, c->p.min_node_size, c->stream, launches));
+    if ((rc = read_counters(c))) return rc;
+    if (c->hcounters[kMcGroups] == 0) return NBODY_OK;
+    uint64_t removed = 0;
+    if ((rc = adopt_compaction(c, fp64, launches, &removed))) return rc;
+    c->merged_min_size += removed;
+    tree_inputs(c, c->n, want_vmax);
+    c->tb.keep_root = 1;
+    cudaError_t e = build_octree(c->tb, c->stream, launches);
+    c->tb.keep_root = 0;
+    NB_CUDA(e);
+    return NBODY_OK;
+}
+
+// Collision capture on the octree of the force pass just run, then the merge.
+int apply_collisions(nbody_ctx *c, unsigned *launches) {
+    if (c->n < 2) return NBODY_OK;
+    int rc = reserve_merge(c);
+    if (rc) return rc;
+    if ((rc = reserve_pairs(c, 4096))) return rc;
+    const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
+    uint32_t np = 0;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        NB_CUDA(merge_begin(c->mb, c->n, c->stream, launches));
+        NB_CUDA(collide_find(c->mb, tree_view(c), c->tb.oparent, c->p.theta, c->p.collision_range, c->stream,
+                             launches));
+        if ((rc = read_counters(c))) return rc;
+        np = c->hcounters[kMcPairs];
+        if (np <= c->mb.pair_cap) break;
+        if ((rc = reserve_pairs(c, np))) return rc;  // found more than fit: grow and search again
+    }
+    c->collision_pairs += np;
+    if (np == 0) return NBODY_OK;
+    if (np > c->mb.pair_cap) return fail(NBODY_ERR_CAPACITY, "collision pairs exceed the buffer%s");
+    NB_CUDA(collide_components(c->mb, c->n, np, c->stream, launches));
+    if ((rc = read_counters(c))) return rc;
+    NB_CUDA(collide_fold(c->mb, c->hcounters[kMcInvolved], c->pos, c->vel, c->mass, c->stream, launches));
+    uint64_t removed = 0;
+    if ((rc = adopt_compaction(c, fp64, launches, &removed))) return rc;
+    c->merged_collisions += removed;
+    if (c->p.adaptive) NB_CUDA(merge_maxima(c->acc, fp64, c->vel, c->n, c->sc, c->stream, launches));
+    return NBODY_OK;
+}
+
 int one_step(nbody_ctx *c) {
     const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
     StepParams sp{c->p.dt, c->p.adaptive, c->p.min_adaptive_dt, c->p.max_pos_change, c->p.max_vel_change};
-    int rc = force_pass(c, c->p.damping, c->p.theta, fp64, c->p.adaptive != 0, c->p.adaptive != 0, false, false);
+    const bool merge = merging(c);
+    int rc = force_pass(c, c->p.damping, c->p.theta, fp64, c->p.adaptive != 0, c->p.adaptive != 0, false, false,
+                        nullptr, false, nullptr, merge);
     if (rc) return rc;
+    if (merge && c->p.collide) {
+        unsigned launches = 0;
+        rc = apply_collisions(c, &launches);
+        c->launches += launches;
+        if (rc) return rc;
+    }
     NB_CUDA(launch_update(c->pos, c->vel, c->acc, fp64, c->n, sp, c->sc, c->stream));
     c->launches++;
     return NBODY_OK;
 }
 
 int run_steps(nbody_ctx *c, uint32_t nsteps) {
-    if (c->use_graphs && !c->timing) {
+    if (c->use_graphs && !c->timing && !merging(c)) {  // merging changes n: launched step by step
         auto key = graph_key(c, 0);
         if (!c->step_exec || key != c->step_key) {
             drop_graph(c->step_exec);
@@ -587,6 +775,9 @@ void nbody_default_params(nbody_params *p) {
     p->precision = NBODY_PRECISION_MIXED;
     p->device = 0;
     p->autotune = 0;
+    p->collide = 0;              // src/main.cpp:1353
+    p->collision_range = 0.01;   // src/main.cpp:1354
+    p->min_node_size = 0.0;      // src/main.cpp:1355
 }
 
 int nbody_create(const nbody_params *p, nbody_ctx **out) {
@@ -645,6 +836,9 @@ int nbody_destroy(nbody_ctx *c) {
     if (c->adj_arena) cudaFree(c->adj_arena);
     if (c->sys_arena) cudaFree(c->sys_arena);
     if (c->img_arena) cudaFree(c->img_arena);
+    if (c->merge_arena) cudaFree(c->merge_arena);
+    if (c->pairs) cudaFree(c->pairs);
+    if (c->hcounters) cudaFreeHost(c->hcounters);
     if (c->sc) cudaFree(c->sc);
     if (c->hsc) cudaFreeHost(c->hsc);
     for (auto &e : c->ev)
@@ -806,6 +1000,15 @@ int nbody_get_particles(nbody_ctx *c, double *pos, double *vel, double *acc) {
     return NBODY_OK;
 }
 
+int nbody_get_masses(nbody_ctx *c, double *mass) {
+    CTX_OR_FAIL(c);
+    if (!c->have_state) return fail(NBODY_ERR_STATE, "no particles set%s");
+    if (!mass) return fail(NBODY_ERR_INVALID, "mass is null%s");
+    NB_CUDA(cudaMemcpyAsync(mass, c->mass, 8 * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
+    NB_CUDA(cudaStreamSynchronize(c->stream));
+    return NBODY_OK;
+}
+
 int nbody_compute_forces(nbody_ctx *c) {
     CTX_OR_FAIL(c);
     if (!c->have_state) return fail(NBODY_ERR_STATE, "no particles set%s");
@@ -822,6 +1025,9 @@ int nbody_compute_forces(nbody_ctx *c) {
 int nbody_step(nbody_ctx *c, uint32_t nsteps) {
     CTX_OR_FAIL(c);
     if (!c->have_state || !c->have_vel) return fail(NBODY_ERR_STATE, "particles with velocities must be set first%s");
+    if (merging(c) && c->nsys > 1)
+        return fail(NBODY_ERR_INVALID, "collisions and min_node_size need a single system%s");
+    c->merged_min_size = c->merged_collisions = c->collision_pairs = 0;
     if (c->n == 0 || nsteps == 0) return NBODY_OK;
     int rc = begin_call(c);
     if (rc) return rc;
@@ -836,6 +1042,8 @@ int nbody_step_host(nbody_ctx *c, uint32_t n, double *pos, double *vel, const do
     CTX_OR_FAIL(c);
     if (n > kMaxParticles) return fail(NBODY_ERR_INVALID, "n exceeds the 2^28 particle limit%s");
     if (n && (!pos || !vel || !mass)) return fail(NBODY_ERR_INVALID, "null array%s");
+    if (merging(c))
+        return fail(NBODY_ERR_INVALID, "merging changes n: use nbody_set_particles, nbody_step, nbody_get_particles%s");
     if (n == 0) return NBODY_OK;
     int rc = upload(c, n, pos, vel, mass);
     if (rc) return rc;
@@ -926,6 +1134,7 @@ int nbody_forward_checkpointed(nbody_ctx *c, uint32_t nsteps, uint32_t every) {
     CTX_OR_FAIL(c);
     if (!c->have_state || !c->have_vel) return fail(NBODY_ERR_STATE, "particles with velocities must be set first%s");
     if (c->p.adaptive) return fail(NBODY_ERR_INVALID, "the adjoint needs a fixed dt (adaptive = 0)%s");
+    if (merging(c)) return fail(NBODY_ERR_INVALID, "the adjoint cannot differentiate through merging%s");
     c->have_fwd = false;
     if (nsteps == 0 || c->n == 0) return NBODY_OK;
     if (every == 0) {

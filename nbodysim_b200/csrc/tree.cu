@@ -21,7 +21,7 @@ namespace nbody {
 // adaptive step.
 __global__ void k_bbox(const double *__restrict__ pos, const double *__restrict__ vel,
                        const double *__restrict__ mass, uint32_t n, double *__restrict__ partial,
-                       DevScalars *sc) {
+                       DevScalars *sc, int keep_root) {
     __shared__ double s_red[7][32];
     __shared__ bool s_last;
     double mn[3] = {INFINITY, INFINITY, INFINITY};
@@ -68,7 +68,10 @@ __global__ void k_bbox(const double *__restrict__ pos, const double *__restrict_
         for (uint32_t b = lane; b < gridDim.x; b += 32) acc = fmin(acc, __ldcg(&partial[7 * b + k]));
         r[k] = warp_min(acc);
     }
-    if (lane == 0) {
+    if (lane == 0 && keep_root) {
+        sc->max_vel_bits = (unsigned long long)__double_as_longlong(-r[6]);
+        sc->ticket = 0;
+    } else if (lane == 0) {
         double lo[3] = {r[0], r[1], r[2]}, hi[3] = {-r[3], -r[4], -r[5]};
         for (int k = 0; k < 3; k++) {
             sc->bbox_min[k] = lo[k];
@@ -557,7 +560,8 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
     if (n == 0) return cudaSuccess;
     const bool multi = tb.nsys > 1;
     // root cube (+ max |v| when requested); one per system when there are several
-    k_bbox<<<tb.bbox_blocks, 256, 0, st>>>(tb.pos, tb.vel_for_max, tb.mass, n, tb.bbox_partial, tb.sc);
+    k_bbox<<<tb.bbox_blocks, 256, 0, st>>>(tb.pos, tb.vel_for_max, tb.mass, n, tb.bbox_partial, tb.sc,
+                                           multi ? 0 : tb.keep_root);
     if (multi) {
         k_bbox_systems<<<tb.nsys, 256, 0, st>>>(tb.pos, tb.mass, tb.sys_start, tb.sys_root, tb.sc);
         L += 1;

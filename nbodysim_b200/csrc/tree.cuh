@@ -10,6 +10,7 @@ struct TreeBuild {
     const double *pos;          // user order, AoS
     const double *mass;
     const double *vel_for_max;  // non-null: also reduce max |v| (adaptive dt)
+    int keep_root;              // rebuild inside the root cube already in sc (single system)
     DevScalars *sc;
     double *bbox_partial;       // 7 * bbox_blocks
     unsigned bbox_blocks;

@@ -104,6 +104,9 @@ class Reference:
                                      C.c_void_p, C.c_void_p]
         L.ref_write_image.argtypes = [C.c_uint, C.c_void_p, C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_int, C.c_int,
                                       C.c_double, C.c_double, C.c_void_p]
+        L.ref_frame_merging.argtypes = [C.c_uint, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int,
+                                        C.c_double, C.c_int, C.c_double, C.c_double, C.c_uint,
+                                        C.POINTER(C.c_uint), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         self.datatype_bytes = L.ref_datatype_bytes()
 
     def generate(self, g: GenParams, n: int):
@@ -133,6 +136,22 @@ class Reference:
         self.lib.ref_run_frames(n, pos.ctypes.data, vel.ctypes.data, mass.ctypes.data, theta, int(damping),
                                 dt, threads, frames, out.ctypes.data if out is not None else None)
         return pos, vel, out
+
+    def frame_merging(self, pos, vel, mass, theta=0.5, damping=False, dt=0.0333, collide=False,
+                      collision_range=0.01, min_size=0.0):
+        """One reference frame with collisions and/or apply_minimum_size; returns the
+        surviving particles (pos, vel, acc, mass) in the set's iteration order."""
+        pos = np.ascontiguousarray(pos, dtype=np.float64); vel = np.ascontiguousarray(vel, dtype=np.float64)
+        mass = np.ascontiguousarray(mass, dtype=np.float64)
+        n = len(mass)
+        po = np.zeros((n, 3)); vo = np.zeros((n, 3)); ao = np.zeros((n, 3)); mo = np.zeros(n)
+        k = C.c_uint(0)
+        self.lib.ref_frame_merging(n, pos.ctypes.data, vel.ctypes.data, mass.ctypes.data, C.c_double(theta),
+                                   int(damping), C.c_double(dt), int(collide), C.c_double(collision_range),
+                                   C.c_double(min_size), n, C.byref(k), po.ctypes.data, vo.ctypes.data,
+                                   ao.ctypes.data, mo.ctypes.data)
+        m = k.value
+        return po[:m], vo[:m], ao[:m], mo[:m]
 
     def write_image(self, pos, width=1920, height=1080, projection=3, color=0, adaptive=False, nonlinear=False,
                     scale=1.0, brightness=255.0):

@@ -255,6 +255,63 @@ int ref_run_frames(unsigned int n, double *pos, double *vel, const double *mass,
     return 0;
 }
 
+/* One frame of main()'s loop with the merging steps on (src/main.cpp:1420-1492,
+ * serial build): gen_root -> apply_minimum_size (when min_size > 0) -> calc_mass
+ * -> calc_com -> barnes_hut_threaded with collision capture (when collide) ->
+ * update_collision -> update_all. The surviving particles come back in the
+ * particle set's iteration order (n_out of them; at most cap are written):
+ * position, velocity, acceleration and mass. Particles the reference erases
+ * without deleting (apply_minimum_size) are left allocated: test use only. */
+int ref_frame_merging(unsigned int n, const double *pos, const double *vel, const double *mass, double theta,
+                      int damping, double dt, int collide, double collision_range, double min_size,
+                      unsigned int cap, unsigned int *n_out, double *pos_out, double *vel_out, double *acc_out,
+                      double *mass_out) {
+    std::vector<particle *> order;
+    particle_set *set = new particle_set;
+    make_particles(n, pos, vel, mass, order, *set);
+    settings cfg;
+    settings_for_walk(cfg, theta, damping, 1);
+    cfg.dt = (datatype)dt;
+    cfg.collide = collide != 0;
+    cfg.collision_range = (datatype)collision_range;
+    cfg.min_node_size = (datatype)min_size;
+    if (n > 0) {
+        octree *root = gen_root(set);
+        if (cfg.min_node_size > 0.0) apply_minimum_size(cfg.min_node_size, root, set, NULL);
+        root->calc_mass();
+        root->calc_com();
+        particle_set *added = NULL, *removed = NULL;
+        if (cfg.collide) {
+            added = new particle_set;
+            removed = new particle_set;
+        }
+        barnes_hut_threaded(cfg, set, root, added, removed);
+        delete root;
+        if (cfg.collide) {
+            update_collision(set, added, removed, false);
+            delete added;
+            delete removed;
+        }
+        update_all(cfg, set);
+    }
+    unsigned int k = 0;
+    for (particle_set::iterator it = set->begin(); it != set->end(); ++it, ++k) {
+        if (k >= cap) continue;
+        particle *q = *it;
+        pos_out[3 * k] = q->get_pos()->get_x(); pos_out[3 * k + 1] = q->get_pos()->get_y();
+        pos_out[3 * k + 2] = q->get_pos()->get_z();
+        vel_out[3 * k] = q->get_vel()->get_x(); vel_out[3 * k + 1] = q->get_vel()->get_y();
+        vel_out[3 * k + 2] = q->get_vel()->get_z();
+        acc_out[3 * k] = q->get_acc()->get_x(); acc_out[3 * k + 1] = q->get_acc()->get_y();
+        acc_out[3 * k + 2] = q->get_acc()->get_z();
+        mass_out[k] = q->get_mass();
+    }
+    *n_out = k;
+    for (particle_set::iterator it = set->begin(); it != set->end(); ++it) delete *it;
+    delete set;
+    return 0;
+}
+
 /* The reference's write_image (src/main.cpp:556-678) on n positions; the
  * rendered 24-bit bitmap comes back through the FreeImage stand-in:
  * rgb_out[(y * w + x) * 3 + {R, G, B}], y as FreeImage counts it (row 0 at the

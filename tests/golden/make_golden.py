@@ -4,7 +4,8 @@ Runs only where the reference tree is present and ``make -C oracle ref`` has
 built ``oracle/_ref/libnbref.so`` (fosted3/nbodysim's src/main.cpp, octree.cpp,
 particle.cpp, vector.cpp compiled unmodified, DOUBLE build). The outputs are
 small ``.npz`` files that pin the oracle (``oracle/bh_oracle.c``) where the
-reference is absent. Usage: ``python tests/golden/make_golden.py``.
+reference is absent. Usage: ``python tests/golden/make_golden.py`` (all), or
+``python tests/golden/make_golden.py merging`` (the merging fixture only).
 """
 from __future__ import annotations
 
@@ -26,9 +27,33 @@ def lattice(k: int, step: float = 1.0):
     return np.ascontiguousarray(g), np.full(len(g), 1e10)
 
 
+MERGE_CASES = (  # name, collide, collision_range, min_size
+    ("collide_0.6", True, 0.6, 0.0),
+    ("collide_1.0", True, 1.0, 0.0),
+    ("minsize_1.0", False, 0.01, 1.0),
+    ("minsize_2.0", False, 0.01, 2.0),
+    ("both", True, 0.6, 2.0),
+)
+
+
+def merging(R) -> None:
+    """One frame with collisions / apply_minimum_size, cube N = 400 in a 20-wide box."""
+    pos, vel, mass = R.generate(O.GenParams(size=20.0), 400)
+    out = dict(pos=pos, vel=vel, mass=mass)
+    for name, collide, rng, ms in MERGE_CASES:
+        p, v, a, m = R.frame_merging(pos, vel, mass, collide=collide, collision_range=rng, min_size=ms)
+        order = np.argsort(m, kind="stable")  # the set's iteration order is arbitrary
+        out[f"{name}_pos"], out[f"{name}_vel"], out[f"{name}_mass"] = p[order], v[order], m[order]
+    np.savez_compressed(os.path.join(HERE, "merge_cube400.npz"), **out)
+
+
 def main() -> None:
     R = O.Reference()
     assert R.datatype_bytes == 8
+    if sys.argv[1:] == ["merging"]:
+        merging(R)
+        return
+    merging(R)
     out = {}
     # seeded initial conditions: 64 particles per gen type x mass distribution
     for gt in (O.CUBE, O.SPHERE, O.SHELL):

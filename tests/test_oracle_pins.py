@@ -106,3 +106,31 @@ def test_reference_image_hand_cases(ref):
     # y between h-1 and w-1 is clamped onto the top row (the bound uses the width)
     im = ref.write_image(np.array([[0.0, 0.0, 4.0]]), 12, 6, 0, 0, False, False, 1.0, 10.0)
     assert im[5, 6].tolist() == [10, 10, 10]
+
+
+def test_reference_merging_hand_cases(ref):
+    """The reference's merging steps on hand-worked layouts (one frame, dt 0.0333)."""
+    import numpy as np
+    dt = 0.0333
+    # A=(0,0,0), B=(0.1,0,0), C=(10,0,0): root side 12, A and B share cells down to
+    # level 6 (side 0.1875) and split at level 7 (side 0.09375)
+    pos = np.array([[0.0, 0, 0], [0.1, 0, 0], [10.0, 0, 0]])
+    vel = np.array([[1.0, 0, 0], [0.0, 2.0, 0], [0.0, 0, 0]])
+    mass = np.array([3e9, 1e9, 5e9])
+    _, _, _, m = ref.frame_merging(pos, vel, mass, min_size=0.1)
+    assert len(m) == 3
+    p, v, a, m = ref.frame_merging(pos, vel, mass, min_size=0.2)
+    assert sorted(m.tolist()) == [4e9, 5e9]
+    k = int(np.argmin(m))
+    vm = (vel[0] * 3e9 + vel[1] * 1e9) / 4e9  # collide(): mass-weighted averages
+    pm = (pos[0] * 3e9 + pos[1] * 1e9) / 4e9
+    # the merged particle feels C's pull before the update; its velocity moves by a * dt
+    assert np.allclose(v[k], vm + a[k] * dt, rtol=0, atol=1e-15)
+    assert np.allclose(p[k], pm + v[k] * dt, rtol=0, atol=1e-15)
+    # collisions: A and B within range 0.2 merge after the forces; the new particle has a = 0
+    p, v, a, m = ref.frame_merging(pos, vel, mass, collide=True, collision_range=0.2)
+    k = int(np.argmin(m))
+    assert len(m) == 2 and m[k] == 4e9 and not a[k].any()
+    assert np.array_equal(v[k], vm) and np.array_equal(p[k], pm + vm * dt)
+    _, _, _, m = ref.frame_merging(pos, vel, mass, collide=True, collision_range=0.05)
+    assert len(m) == 3
