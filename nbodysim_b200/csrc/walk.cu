@@ -231,47 +231,63 @@ __device__ inline void pair_adjoint(T dx, T dy, T dz, T r2, T gm, T lax, T lay, 
     mterm = T(kG) * g * s;
 }
 
-// Sums four per-lane values over the warp in six shuffles; lane 0 ends with
-// the sum of a, lane 8 of b, lane 16 of c, lane 24 of d.
+// Sums 32 per-lane values over the warp: lane l returns the sum over lanes of
+// v[l]. Five butterfly stages (16 + 8 + 4 + 2 + 1 shuffles); at each stage a
+// lane keeps the half of its values whose index has its own lane bit and sends
+// the other half to its partner, so the 32 sums come out one per lane with
+// only five dependent shuffles.
 template <typename T>
-__device__ inline T warp_sum4(T a, T b, T c, T d, int lane) {
-    const bool h16 = lane & 16;
-    T x0 = h16 ? c : a, x1 = h16 ? d : b;
-    const T y0 = h16 ? a : c, y1 = h16 ? b : d;
-    x0 += __shfl_xor_sync(0xffffffffu, y0, 16);
-    x1 += __shfl_xor_sync(0xffffffffu, y1, 16);
-    const bool h8 = lane & 8;
-    T z = h8 ? x1 : x0;
-    const T w = h8 ? x0 : x1;
-    z += __shfl_xor_sync(0xffffffffu, w, 8);
-    z += __shfl_xor_sync(0xffffffffu, z, 4);
-    z += __shfl_xor_sync(0xffffffffu, z, 2);
-    z += __shfl_xor_sync(0xffffffffu, z, 1);
-    return z;
+__device__ inline T warp_transpose_sum32(T (&v)[32], int lane) {
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        const bool h = lane & o;
+#pragma unroll
+        for (int i = 0; i < o; i++) {
+            const T send = h ? v[i] : v[i + o];
+            const T keep = h ? v[i + o] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    return v[0];
 }
 
-__device__ inline void scatter_adj(double *adj_node, double *adj_leaf, int ref, double z, int lane) {
-    if ((lane & 7) == 0) {
+// Lane l holds the warp sum of component (l & 3) of entry (l >> 2) of a chunk of
+// eight: adds it to that node's (or leaf's) cotangent (x, y, z, mass).
+__device__ inline void scatter_adj8(double *adj_node, double *adj_leaf, const int *lr, int k0, int count, double z,
+                                    int lane) {
+    const int k = k0 + (lane >> 2);
+    if (k < count) {
+        const int ref = lr[k];
         double *dst = ref >= 0 ? adj_node + 4 * (size_t)ref : adj_leaf + 4 * (size_t)(~ref);
-        atomicAdd(dst + (lane >> 3), z);
+        atomicAdd(dst + (lane & 3), z);
     }
 }
 
+// The list in chunks of eight entries: every lane's pair terms for the chunk,
+// one transposed warp reduction, one atomic per lane.
 template <bool kDamp>
 __device__ inline void adj_list_f32(const float4 *lc, const uint32_t *lm, const int *lr, int count, int lane,
                                     float px, float py, float pz, float lax, float lay, float laz, float &gx,
                                     float &gy, float &gz, double *adj_node, double *adj_leaf) {
-    for (int k = 0; k < count; k++) {
-        const float4 c = lc[k];
-        const bool take = (lm[k] >> lane) & 1u;
-        const float dx = c.x - px, dy = c.y - py, dz = c.z - pz;
-        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-        float vx, vy, vz, mt;
-        pair_adjoint<kDamp, float>(dx, dy, dz, r2, c.w, lax, lay, laz, vx, vy, vz, mt);
-        if (!take) vx = vy = vz = mt = 0.f;
-        gx -= vx; gy -= vy; gz -= vz;
-        const float z = warp_sum4(vx, vy, vz, mt, lane);
-        scatter_adj(adj_node, adj_leaf, lr[k], (double)z, lane);
+    for (int k0 = 0; k0 < count; k0 += 8) {
+        float v[32];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int k = k0 + j;
+            float vx = 0.f, vy = 0.f, vz = 0.f, mt = 0.f;
+            if (k < count) {
+                const float4 c = lc[k];
+                const bool take = (lm[k] >> lane) & 1u;
+                const float dx = c.x - px, dy = c.y - py, dz = c.z - pz;
+                const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                pair_adjoint<kDamp, float>(dx, dy, dz, r2, c.w, lax, lay, laz, vx, vy, vz, mt);
+                if (!take) vx = vy = vz = mt = 0.f;
+            }
+            gx -= vx; gy -= vy; gz -= vz;
+            v[4 * j] = vx; v[4 * j + 1] = vy; v[4 * j + 2] = vz; v[4 * j + 3] = mt;
+        }
+        const float z = warp_transpose_sum32(v, lane);
+        scatter_adj8(adj_node, adj_leaf, lr, k0, count, (double)z, lane);
     }
 }
 
@@ -279,18 +295,23 @@ template <bool kDamp>
 __device__ inline void adj_near_f32(const double4 *nc, const uint32_t *nm, const int *nr, int count, int lane,
                                     double bx, double by, double bz, float lax, float lay, float laz, float &gx,
                                     float &gy, float &gz, double *adj_node, double *adj_leaf) {
-    for (int k = 0; k < count; k++) {
-        const double4 c = nc[k];
-        const bool take = (nm[k] >> lane) & 1u;
-        float vx = 0.f, vy = 0.f, vz = 0.f, mt = 0.f;
-        if (take) {
-            const float dx = (float)(c.x - bx), dy = (float)(c.y - by), dz = (float)(c.z - bz);
-            const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-            pair_adjoint<kDamp, float>(dx, dy, dz, r2, (float)c.w, lax, lay, laz, vx, vy, vz, mt);
+    for (int k0 = 0; k0 < count; k0 += 8) {
+        float v[32];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int k = k0 + j;
+            float vx = 0.f, vy = 0.f, vz = 0.f, mt = 0.f;
+            if (k < count && ((nm[k] >> lane) & 1u)) {
+                const double4 c = nc[k];
+                const float dx = (float)(c.x - bx), dy = (float)(c.y - by), dz = (float)(c.z - bz);
+                const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                pair_adjoint<kDamp, float>(dx, dy, dz, r2, (float)c.w, lax, lay, laz, vx, vy, vz, mt);
+            }
+            gx -= vx; gy -= vy; gz -= vz;
+            v[4 * j] = vx; v[4 * j + 1] = vy; v[4 * j + 2] = vz; v[4 * j + 3] = mt;
         }
-        gx -= vx; gy -= vy; gz -= vz;
-        const float z = warp_sum4(vx, vy, vz, mt, lane);
-        scatter_adj(adj_node, adj_leaf, nr[k], (double)z, lane);
+        const float z = warp_transpose_sum32(v, lane);
+        scatter_adj8(adj_node, adj_leaf, nr, k0, count, (double)z, lane);
     }
 }
 
@@ -298,18 +319,23 @@ template <bool kDamp>
 __device__ inline void adj_list_f64(const double4 *lc, const uint32_t *lm, const int *lr, int count, int lane,
                                     double bx, double by, double bz, double lax, double lay, double laz, double &gx,
                                     double &gy, double &gz, double *adj_node, double *adj_leaf) {
-    for (int k = 0; k < count; k++) {
-        const double4 c = lc[k];
-        const bool take = (lm[k] >> lane) & 1u;
-        double vx = 0.0, vy = 0.0, vz = 0.0, mt = 0.0;
-        if (take) {
-            const double dx = c.x - bx, dy = c.y - by, dz = c.z - bz;
-            const double r2 = dx * dx + dy * dy + dz * dz;
-            pair_adjoint<kDamp, double>(dx, dy, dz, r2, c.w, lax, lay, laz, vx, vy, vz, mt);
+    for (int k0 = 0; k0 < count; k0 += 8) {
+        double v[32];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int k = k0 + j;
+            double vx = 0.0, vy = 0.0, vz = 0.0, mt = 0.0;
+            if (k < count && ((lm[k] >> lane) & 1u)) {
+                const double4 c = lc[k];
+                const double dx = c.x - bx, dy = c.y - by, dz = c.z - bz;
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                pair_adjoint<kDamp, double>(dx, dy, dz, r2, c.w, lax, lay, laz, vx, vy, vz, mt);
+            }
+            gx -= vx; gy -= vy; gz -= vz;
+            v[4 * j] = vx; v[4 * j + 1] = vy; v[4 * j + 2] = vz; v[4 * j + 3] = mt;
         }
-        gx -= vx; gy -= vy; gz -= vz;
-        const double z = warp_sum4(vx, vy, vz, mt, lane);
-        scatter_adj(adj_node, adj_leaf, lr[k], z, lane);
+        const double z = warp_transpose_sum32(v, lane);
+        scatter_adj8(adj_node, adj_leaf, lr, k0, count, z, lane);
     }
 }
 
