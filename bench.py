@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU walk seconds of the sample")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-configs", action="store_true", help="skip the cube / sphere / theta-sweep legs")
     ap.add_argument("--adjoint-fd", type=int, default=0,
                     help="also check the config-4 gradient against central differences on this many coordinates")
     return ap.parse_args()
@@ -315,6 +316,13 @@ def run_ours(args) -> None:
     if not args.no_ensemble:
         ensemble = ensemble_leg(nb, torch, stream, local)
 
+    # ---- the other configurations: cube 5000 x 300 frames, sphere 100k x 100 steps, theta sweep at 1M
+    configs = None
+    if not args.no_configs:
+        configs = {"cube5000": cube_leg(nb, torch, stream, local),
+                   "sphere100k": sphere_leg(nb, torch, stream, local),
+                   "shell1M_theta": theta_leg(nb, torch, stream, local, pos0, vel0, mass)}
+
     # ---- accuracy on the initial state: vs the FP64 form (same lists) and FP64 direct sum
     acc_mixed, counts = eng.barnes_hut(pos0, mass, theta=args.theta, counts=True)
     with nb.Engine(nb.default_params(theta=args.theta, precision=nb.PRECISION_FP64, device=local)) as e64:
@@ -375,6 +383,7 @@ def run_ours(args) -> None:
         "adjoint_fwd_ratio": adjoint["ratio"] if adjoint else None,
         "adjoint": adjoint,
         "ensemble": ensemble,
+        "configs": configs,
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 56 * args.n,
                 "d2h_bytes_per_step": 48 * args.n},
@@ -443,6 +452,113 @@ def adjoint_leg(nb, torch, stream, device, fd_coords=0):
                 rel.append(abs(fd - gp[p, k]) / max(abs(fd), abs(gp[p, k]), 1e-300))
             out["fd_check"] = {"coords": fd_coords, "eps": "1e-3 relative", "median_rel": float(np.median(rel)),
                                "max_rel": float(np.max(rel)), "frac_le_1e-4": float(np.mean(np.array(rel) <= 1e-4))}
+    return out
+
+
+def _timed_steps(eng, torch, stream, steps):
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    eng.step(steps)
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b)
+
+
+def cube_leg(nb, torch, stream, device, frames=300):
+    """Config 1: cube N=5000, size 512, masses U[5e10, 5e11], zero velocities,
+    seed 0xDEADBEEF, theta 0.5, dt 0.0333, 300 frames. Final positions against
+    the reference's own frame loop (oracle/_ref, serial build) where it is built."""
+    pos, vel, mass = nb.generate(5000, gen_type=0, size=512.0, seed=0xDEADBEEF)
+    out = {"config": "cube N=5000 size=512 theta=0.5 dt=0.0333, 300 frames"}
+    finals = {}
+    for name, prec in (("mixed", nb.PRECISION_MIXED), ("fp64_form", nb.PRECISION_FP64)):
+        with nb.Engine(nb.default_params(precision=prec, device=device)) as e:
+            e._lib.nbody_set_stream(e._h, C_void(stream.cuda_stream))
+            e.set_particles(pos, vel, mass)
+            e.step(3)
+            ms = _timed_steps(e, torch, stream, frames)
+            e.set_particles(pos, vel, mass)
+            e.step(frames)
+            finals[name] = e.get_particles()[0]
+        out[name] = {"ms_per_step": ms / frames, "steps_per_s": 1e3 * frames / ms}
+    try:
+        import oracle
+        import time
+        R = oracle.Reference()
+        t0 = time.perf_counter()
+        ref_pos, _, _ = R.run_frames(pos, vel, mass, frames, threads=1)
+        t1 = time.perf_counter()
+        scale = np.abs(ref_pos).max()
+        for name in finals:
+            out[name]["max_pos_err_vs_reference"] = float(np.abs(finals[name] - ref_pos).max() / scale)
+        out["reference_cpu"] = {"steps_per_s": frames / (t1 - t0), "cores": 1, "kind": "reference"}
+    except Exception as ex:  # the reference harness is optional on the box
+        out["reference_cpu"] = {"unavailable": str(ex)}
+    return out
+
+
+def sphere_leg(nb, torch, stream, device, steps=100):
+    """Config 2: sphere N=100,000, r 100, masses U[5e10, 5e11], rotation 0.1 about z,
+    size 512, theta 0.5, dt 0.0333, 100 steps: steps/s and energy drift of the MIXED
+    form next to the FP64 form; error against an FP64 direct sum on a 4096-particle
+    subsample (numpy default_rng(0xDEADBEEF))."""
+    pos, vel, mass = nb.generate(100000, gen_type=1, size=512.0, r_sphere=100.0, rotation_magnitude=0.1,
+                                 seed=0xDEADBEEF)
+    out = {"config": "sphere N=100000 r=100 rotation 0.1 theta=0.5 dt=0.0333, 100 steps"}
+    accs = {}
+    for name, prec in (("mixed", nb.PRECISION_MIXED), ("fp64_form", nb.PRECISION_FP64)):
+        with nb.Engine(nb.default_params(precision=prec, device=device)) as e:
+            e._lib.nbody_set_stream(e._h, C_void(stream.cuda_stream))
+            accs[name] = e.barnes_hut(pos, mass)
+            e.set_particles(pos, vel, mass)
+            d0 = e.diagnostics()
+            e.step(steps)
+            d1 = e.diagnostics()
+            e.set_particles(pos, vel, mass)
+            e.step(3)
+            ms = _timed_steps(e, torch, stream, steps)
+        E0 = d0["kinetic"] + d0["potential"]
+        E1 = d1["kinetic"] + d1["potential"]
+        P0 = np.linalg.norm(d0["momentum"])
+        out[name] = {"ms_per_step": ms / steps, "steps_per_s": 1e3 * steps / ms,
+                     "energy_drift": (E1 - E0) / abs(E0),
+                     "momentum_change": float(np.linalg.norm(np.subtract(d1["momentum"], d0["momentum"]))
+                                              / max(P0, float(np.sum(mass)) * 1e-30))}
+    try:
+        import oracle
+        idx = np.random.default_rng(0xDEADBEEF).choice(len(mass), 4096, replace=False)
+        d = oracle.Oracle().direct(pos, mass, targets=idx)
+        nrm = np.linalg.norm(d, axis=1)
+        for name, a in accs.items():
+            out[name]["p99_err_vs_direct_sum"] = float(np.percentile(np.linalg.norm(a[idx] - d, axis=1) / nrm, 99))
+        out["mixed"]["p99_err_vs_fp64_form"] = float(np.percentile(
+            np.linalg.norm(accs["mixed"] - accs["fp64_form"], axis=1) / np.linalg.norm(accs["fp64_form"], axis=1), 99))
+    except Exception as ex:
+        out["direct_sum"] = {"unavailable": str(ex)}
+    return out
+
+
+def theta_leg(nb, torch, stream, device, pos, vel, mass, steps=10):
+    """Config 3 at theta 0.3 / 0.5 / 0.7: 10 adaptive-dt steps from the initial
+    state (autotuned), and the MIXED error against the FP64 form on that state."""
+    out = {}
+    for theta in (0.3, 0.5, 0.7):
+        p = nb.default_params(theta=theta, adaptive=1, min_adaptive_dt=0.00333, max_pos_change=3.0,
+                              max_vel_change=3.0, device=device, autotune=1)
+        with nb.Engine(p) as e:
+            e._lib.nbody_set_stream(e._h, C_void(stream.cuda_stream))
+            acc = e.barnes_hut(pos, mass, theta=theta)
+            e.set_particles(pos, vel, mass)
+            e.step(2)
+            e.set_particles(pos, vel, mass)
+            ms = _timed_steps(e, torch, stream, steps)
+            inter = e.stats()["interactions_total"]
+        with nb.Engine(nb.default_params(theta=theta, precision=nb.PRECISION_FP64, device=device)) as e64:
+            acc64 = e64.barnes_hut(pos, mass, theta=theta)
+        rel = np.linalg.norm(acc - acc64, axis=1) / np.linalg.norm(acc64, axis=1)
+        out[str(theta)] = {"ms_per_step": ms / steps, "interactions_per_step": inter / steps,
+                           "interactions_per_s": inter / (ms * 1e-3), "p99_err_vs_fp64_form": float(np.percentile(rel, 99))}
     return out
 
 
