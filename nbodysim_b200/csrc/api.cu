@@ -50,6 +50,7 @@ constexpr uint32_t kMaxParticles = 1u << 28;
 constexpr uint32_t kSpillCap = 4096;  // entries per walk warp
 constexpr unsigned kBboxBlocks = 592;
 constexpr unsigned kDiagBlocks = 296;
+constexpr uint32_t kOverlapMin = 65536;  // nbody_step_host overlaps the velocity upload from this size
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -115,6 +116,9 @@ struct nbody_ctx {
     uint2 *pairs = nullptr;
     uint32_t *hcounters = nullptr;  // pinned mirror of mb.counters
     uint64_t merged_min_size = 0, merged_collisions = 0, collision_pairs = 0;
+    // nbody_step_host: velocities uploaded on a second stream while the tree is built
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_vel = nullptr;
 };
 
 namespace {
@@ -566,7 +570,10 @@ int apply_collisions(nbody_ctx *c, unsigned *launches) {
     uint64_t removed = 0;
     if ((rc = adopt_compaction(c, fp64, launches, &removed))) return rc;
     c->merged_collisions += removed;
-    if (c->p.adaptive) NB_CUDA(merge_maxima(c->acc, fp64, c->vel, c->n, c->sc, c->stream, launches));
+    if (c->p.adaptive) {
+        NB_CUDA(launch_maxima(c->acc, fp64, c->vel, c->n, c->sc, c->stream));
+        *launches += 1;
+    }
     return NBODY_OK;
 }
 
@@ -653,16 +660,6 @@ int adjoint_force(nbody_ctx *c, const double *pos, int damping, double theta, bo
     if (rc) return rc;
     NB_CUDA(launch_adj_distribute(c->tb.body, c->tb.idx_a, c->tb.leaf_oparent, c->tb.oparent, c->tb.onode,
                                   c->adj_node, c->adj_leaf, c->gdir, fp64, c->lx, c->lm, c->n, c->stream));
-    c->launches++;
-    return NBODY_OK;
-}
-
-// One forward step on explicit buffers (recomputation inside a segment).
-int step_on(nbody_ctx *c, double *pos, double *vel, bool fp64) {
-    StepParams sp{c->p.dt, 0, 0, 0, 0};
-    int rc = force_pass(c, c->p.damping, c->p.theta, fp64, false, false, false, false, pos, false);
-    if (rc) return rc;
-    NB_CUDA(launch_update(pos, vel, c->acc, fp64, c->n, sp, c->sc, c->stream));
     c->launches++;
     return NBODY_OK;
 }
@@ -839,6 +836,9 @@ int nbody_destroy(nbody_ctx *c) {
     if (c->merge_arena) cudaFree(c->merge_arena);
     if (c->pairs) cudaFree(c->pairs);
     if (c->hcounters) cudaFreeHost(c->hcounters);
+    if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_vel) cudaEventDestroy(c->ev_vel);
     if (c->sc) cudaFree(c->sc);
     if (c->hsc) cudaFreeHost(c->hsc);
     for (auto &e : c->ev)
@@ -1045,11 +1045,44 @@ int nbody_step_host(nbody_ctx *c, uint32_t n, double *pos, double *vel, const do
     if (merging(c))
         return fail(NBODY_ERR_INVALID, "merging changes n: use nbody_set_particles, nbody_step, nbody_get_particles%s");
     if (n == 0) return NBODY_OK;
-    int rc = upload(c, n, pos, vel, mass);
-    if (rc) return rc;
-    c->have_vel = true;
-    if ((rc = begin_call(c))) return rc;
-    if ((rc = run_steps(c, nsteps))) return rc;
+    int rc;
+    if (n >= kOverlapMin && nsteps > 0) {
+        // Positions and masses first (the tree needs them); the velocities cross
+        // on a second stream while the first force pass runs, and are waited for
+        // just before that step's update.
+        if ((rc = reserve(c, n))) return rc;
+        if (!c->aux_stream) {
+            NB_CUDA(cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking));
+            NB_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+            NB_CUDA(cudaEventCreateWithFlags(&c->ev_vel, cudaEventDisableTiming));
+        }
+        NB_CUDA(cudaEventRecord(c->ev_fork, c->stream));
+        NB_CUDA(cudaStreamWaitEvent(c->aux_stream, c->ev_fork, 0));
+        NB_CUDA(cudaMemcpyAsync(c->vel, vel, 24 * (size_t)n, cudaMemcpyHostToDevice, c->aux_stream));
+        NB_CUDA(cudaEventRecord(c->ev_vel, c->aux_stream));
+        NB_CUDA(cudaMemcpyAsync(c->pos, pos, 24 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+        NB_CUDA(cudaMemcpyAsync(c->mass, mass, 8 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+        c->n = n;
+        c->have_state = c->have_vel = true;
+        c->have_acc = false;
+        if ((rc = begin_call(c))) return rc;
+        const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
+        StepParams sp{c->p.dt, c->p.adaptive, c->p.min_adaptive_dt, c->p.max_pos_change, c->p.max_vel_change};
+        if ((rc = force_pass(c, c->p.damping, c->p.theta, fp64, false, false, false, false))) return rc;
+        NB_CUDA(cudaStreamWaitEvent(c->stream, c->ev_vel, 0));
+        if (c->p.adaptive) {
+            NB_CUDA(launch_maxima(c->acc, fp64, c->vel, n, c->sc, c->stream));
+            c->launches++;
+        }
+        NB_CUDA(launch_update(c->pos, c->vel, c->acc, fp64, n, sp, c->sc, c->stream));
+        c->launches++;
+        if (nsteps > 1 && (rc = run_steps(c, nsteps - 1))) return rc;
+    } else {
+        if ((rc = upload(c, n, pos, vel, mass))) return rc;
+        c->have_vel = true;
+        if ((rc = begin_call(c))) return rc;
+        if ((rc = run_steps(c, nsteps))) return rc;
+    }
     NB_CUDA(cudaMemcpyAsync(pos, c->pos, 24 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
     NB_CUDA(cudaMemcpyAsync(vel, c->vel, 24 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
     if ((rc = copy_scalars_back(c))) return rc;
@@ -1242,12 +1275,12 @@ int nbody_save_frame(nbody_ctx *c, const char *dir, uint32_t frame, int binary, 
     if (binary) {
         if (nbody_frame_path(dir, frame, 1, path, sizeof path) ||
             nbody_write_dat(path, c->n, pos.data(), vel.data(), acc.data(), mass.data(), datatype_bytes))
-            return fail(NBODY_ERR_INVALID, "cannot write binary frame %s", path);
+            return fail(NBODY_ERR_INVALID, "cannot write binary frame %.400s", path);
     }
     if (text) {
         if (nbody_frame_path(dir, frame, 0, path, sizeof path) ||
             nbody_write_txt(path, c->n, pos.data(), datatype_bytes))
-            return fail(NBODY_ERR_INVALID, "cannot write text frame %s", path);
+            return fail(NBODY_ERR_INVALID, "cannot write text frame %.400s", path);
     }
     return NBODY_OK;
 }
@@ -1265,10 +1298,10 @@ int nbody_load_frame(nbody_ctx *c, const char *dir, uint32_t num_frames, int dat
     uint32_t n = 0;
     if (nbody_frame_path(dir, (uint32_t)f, 1, path, sizeof path) ||
         nbody_read_dat(path, datatype_bytes, &n, nullptr, nullptr, nullptr, nullptr))
-        return fail(NBODY_ERR_INVALID, "cannot read %s", path);
+        return fail(NBODY_ERR_INVALID, "cannot read %.400s", path);
     std::vector<double> pos(3 * (size_t)n), vel(3 * (size_t)n), mass(n);
     if (nbody_read_dat(path, datatype_bytes, &n, pos.data(), vel.data(), nullptr, mass.data()))
-        return fail(NBODY_ERR_INVALID, "cannot read %s", path);
+        return fail(NBODY_ERR_INVALID, "cannot read %.400s", path);
     int rc = nbody_set_particles(c, n, pos.data(), vel.data(), mass.data());
     if (rc) return rc;
     *next_frame = (uint32_t)f + 1;

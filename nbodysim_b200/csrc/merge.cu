@@ -301,24 +301,6 @@ __global__ void k_compact(MergeBufs m, uint32_t n, const double *__restrict__ po
     }
 }
 
-template <typename AccT>
-__global__ void k_maxima(const AccT *__restrict__ acc, const double *__restrict__ vel, uint32_t n, DevScalars *sc) {
-    double amax = 0.0, vmax = 0.0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const size_t o = 3 * (size_t)i;
-        const double ax = acc[o], ay = acc[o + 1], az = acc[o + 2];
-        const double vx = vel[o], vy = vel[o + 1], vz = vel[o + 2];
-        amax = fmax(amax, sqrt(ax * ax + ay * ay + az * az));
-        vmax = fmax(vmax, sqrt(vx * vx + vy * vy + vz * vz));
-    }
-    amax = warp_max(amax);
-    vmax = warp_max(vmax);
-    if ((threadIdx.x & 31) == 0) {
-        atomic_max_nonneg(&sc->max_acc_bits, amax);
-        atomic_max_nonneg(&sc->max_vel_bits, vmax);
-    }
-}
-
 inline unsigned blocks_for(uint64_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
@@ -383,18 +365,6 @@ cudaError_t merge_compact(const MergeBufs &m, uint32_t n, const double *pos, con
     *launches += 1 + scan_exclusive(m.offs, n, m.scan_tmp, &m.counters[kMcKept], st);
     if (acc_double) k_compact<double><<<blocks_for(n, 256), 256, 0, st>>>(m, n, pos, vel, mass, (const double *)acc);
     else k_compact<float><<<blocks_for(n, 256), 256, 0, st>>>(m, n, pos, vel, mass, (const float *)acc);
-    *launches += 1;
-    return cudaGetLastError();
-}
-
-cudaError_t merge_maxima(const void *acc, bool acc_double, const double *vel, uint32_t n, DevScalars *sc,
-                         cudaStream_t st, unsigned *launches) {
-    cudaError_t e = cudaMemsetAsync(&sc->max_acc_bits, 0, sizeof(unsigned long long), st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(&sc->max_vel_bits, 0, sizeof(unsigned long long), st);
-    if (e != cudaSuccess || n == 0) return e;
-    const unsigned blocks = std::min(blocks_for(n, 256), 592u);
-    if (acc_double) k_maxima<double><<<blocks, 256, 0, st>>>((const double *)acc, vel, n, sc);
-    else k_maxima<float><<<blocks, 256, 0, st>>>((const float *)acc, vel, n, sc);
     *launches += 1;
     return cudaGetLastError();
 }

@@ -66,8 +66,4 @@ cudaError_t collide_fold(const MergeBufs &m, uint32_t k, const double *pos, cons
 cudaError_t merge_compact(const MergeBufs &m, uint32_t n, const double *pos, const double *vel, const double *mass,
                           const void *acc, bool acc_double, cudaStream_t st, unsigned *launches);
 
-// max |a| and max |v| over n particles into sc (adaptive dt after merging).
-cudaError_t merge_maxima(const void *acc, bool acc_double, const double *vel, uint32_t n, DevScalars *sc,
-                         cudaStream_t st, unsigned *launches);
-
 }  // namespace nbody

@@ -1,6 +1,8 @@
 // Integration step, adaptive dt and FP64 diagnostics.
 #include "step.cuh"
 
+#include <algorithm>
+
 namespace nbody {
 
 // Semi-implicit Euler exactly as particle::update (src/particle.cpp:66-74):
@@ -205,6 +207,38 @@ cudaError_t launch_update(double *pos, double *vel, const void *acc, bool acc_do
 cudaError_t launch_diag(const double *pos, const double *vel, const double *mass, const double *pot,
                         uint32_t n, double *partial, unsigned blocks, DevScalars *sc, cudaStream_t st) {
     k_diag<<<blocks, 256, 0, st>>>(pos, vel, mass, pot, n, partial, sc);
+    return cudaGetLastError();
+}
+
+// max |a| and max |v| over n particles, recomputed into sc (adaptive dt when
+// the walk's running maximum does not apply: after merging, or when the
+// velocities arrive after the force pass).
+template <typename AccT>
+__global__ void k_maxima(const AccT *__restrict__ acc, const double *__restrict__ vel, uint32_t n, DevScalars *sc) {
+    double amax = 0.0, vmax = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const size_t o = 3 * (size_t)i;
+        const double ax = acc[o], ay = acc[o + 1], az = acc[o + 2];
+        const double vx = vel[o], vy = vel[o + 1], vz = vel[o + 2];
+        amax = fmax(amax, sqrt(ax * ax + ay * ay + az * az));
+        vmax = fmax(vmax, sqrt(vx * vx + vy * vy + vz * vz));
+    }
+    amax = warp_max(amax);
+    vmax = warp_max(vmax);
+    if ((threadIdx.x & 31) == 0) {
+        atomic_max_nonneg(&sc->max_acc_bits, amax);
+        atomic_max_nonneg(&sc->max_vel_bits, vmax);
+    }
+}
+
+cudaError_t launch_maxima(const void *acc, bool acc_double, const double *vel, uint32_t n, DevScalars *sc,
+                          cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(&sc->max_acc_bits, 0, sizeof(unsigned long long), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(&sc->max_vel_bits, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess || n == 0) return e;
+    const unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 592);
+    if (acc_double) k_maxima<double><<<blocks, 256, 0, st>>>((const double *)acc, vel, n, sc);
+    else k_maxima<float><<<blocks, 256, 0, st>>>((const float *)acc, vel, n, sc);
     return cudaGetLastError();
 }
 

@@ -18,6 +18,8 @@ cudaError_t launch_update(double *pos, double *vel, const void *acc, bool acc_do
 cudaError_t launch_diag(const double *pos, const double *vel, const double *mass, const double *pot,
                         uint32_t n, double *partial, unsigned blocks, DevScalars *sc, cudaStream_t st);
 cudaError_t launch_reset_pass(DevScalars *sc, cudaStream_t st);
+cudaError_t launch_maxima(const void *acc, bool acc_double, const double *vel, uint32_t n, DevScalars *sc,
+                          cudaStream_t st);
 cudaError_t launch_acc_to_double(const float *in, double *out, size_t count, cudaStream_t st);
 cudaError_t launch_double_to_float(const double *in, float *out, size_t count, cudaStream_t st);
 cudaError_t launch_adj_pre(const double *lx, double *lv, void *lam, bool lam_double, double dt, uint32_t n,

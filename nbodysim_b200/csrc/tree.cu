@@ -504,42 +504,41 @@ __global__ void k_com(const double4 *__restrict__ body, const int32_t *__restric
         uint32_t old = atomicAdd(&ocount[p], 1u);
         if (old != (uint32_t)(nch - 1)) return;
         __threadfence();  // acquire: the other children's results are visible
+        // The reference sums the masses, then the mass-weighted centres, each in
+        // child order; both sums run here in one pass over the children.
         const int L = meta_level(meta);
-        double cm[8];
-        double3 cc[8];
-        double m = 0.0;
+        double m = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
         for (int k = 0; k < nch; k++) {
-            int c = ochild[8 * p + k];
+            const int c = ochild[8 * p + k];
+            double cmk;
+            double3 cck;
             if (c < 0) {
-                double4 b = body[~c];
-                cm[k] = b.w;
-                cc[k] = make_double3(b.x, b.y, b.z);
+                const double4 b = body[~c];
+                cmk = b.w;
+                cck = make_double3(b.x, b.y, b.z);
             } else {
-                cc[k] = load_node_com(&onode[c], cm[k]);
-                int chain = meta_level(ometa[c]) - L - 1;
+                cck = load_node_com(&onode[c], cmk);
+                const int chain = meta_level(ometa[c]) - L - 1;
                 for (int t = 0; t < chain; t++) {
-                    if (cm[k] == 0.0) {
-                        cc[k] = make_double3(0.0, 0.0, 0.0);
+                    if (cmk == 0.0) {
+                        cck = make_double3(0.0, 0.0, 0.0);
                     } else {
-                        cc[k].x = __ddiv_rn(__dmul_rn(cc[k].x, cm[k]), cm[k]);
-                        cc[k].y = __ddiv_rn(__dmul_rn(cc[k].y, cm[k]), cm[k]);
-                        cc[k].z = __ddiv_rn(__dmul_rn(cc[k].z, cm[k]), cm[k]);
+                        cck.x = __ddiv_rn(__dmul_rn(cck.x, cmk), cmk);
+                        cck.y = __ddiv_rn(__dmul_rn(cck.y, cmk), cmk);
+                        cck.z = __ddiv_rn(__dmul_rn(cck.z, cmk), cmk);
                     }
                 }
             }
-            m = __dadd_rn(m, cm[k]);
+            m = __dadd_rn(m, cmk);
+            sx = __dadd_rn(sx, __dmul_rn(cck.x, cmk));
+            sy = __dadd_rn(sy, __dmul_rn(cck.y, cmk));
+            sz = __dadd_rn(sz, __dmul_rn(cck.z, cmk));
         }
         double4 out;
         out.w = m;
         if (m == 0.0) {
             out.x = out.y = out.z = 0.0;
         } else {
-            double sx = 0.0, sy = 0.0, sz = 0.0;
-            for (int k = 0; k < nch; k++) {
-                sx = __dadd_rn(sx, __dmul_rn(cc[k].x, cm[k]));
-                sy = __dadd_rn(sy, __dmul_rn(cc[k].y, cm[k]));
-                sz = __dadd_rn(sz, __dmul_rn(cc[k].z, cm[k]));
-            }
             out.x = __ddiv_rn(sx, m);
             out.y = __ddiv_rn(sy, m);
             out.z = __ddiv_rn(sz, m);

@@ -28,6 +28,23 @@ def test_frames_match_oracle_mixed(nb, orc):
     assert err <= 1e-6 * np.abs(frames[-1]).max(), err
 
 
+@pytest.mark.parametrize("adaptive", [0, 1])
+def test_step_host_overlapped_upload_equals_resident(nb, adaptive):
+    """From 65,536 particles nbody_step_host uploads the velocities on a second
+    stream during the force pass; the result must not change."""
+    pos, vel, mass = nb.generate(70000, gen_type=1, min_vel=0.0, max_vel=2.0)
+    with nb.Engine(adaptive=adaptive) as e:
+        e.set_particles(pos, vel, mass)
+        e.step(2)
+        p1, v1 = e.get_particles()
+        dt1 = e.stats()["last_dt"]
+        p2, v2 = pos.copy(), vel.copy()
+        e.step_host(p2, v2, mass, 1)
+        e.step_host(p2, v2, mass, 1)
+        dt2 = e.stats()["last_dt"]
+    assert np.array_equal(p1, p2) and np.array_equal(v1, v2) and dt1 == dt2
+
+
 def test_step_host_equals_resident(nb):
     pos, vel, mass = nb.generate(3000, gen_type=1)
     with nb.Engine() as e:
