@@ -56,12 +56,22 @@ __device__ inline double exp2_neg(int L) {  // exactly 2^-L for 0 <= L <= 1022
 template <bool kFp64>
 struct WarpSmem;
 
+// Values that are the same for every lane of a group, kept in shared memory
+// rather than in one register per lane.
+struct GroupConsts {
+    double ref[3];      // reference point: centre of the group's bounding box
+    double S, s_theta;  // root side, root side / theta
+    float box[6];       // group box of the FP32 offsets: lo x, hi x, lo y, hi y, lo z, hi z
+    float pm_tol, tiny, near_r2, pad;
+    uint32_t st[6];     // per-group statistics: entries, tiles, decisions, list, near, deepest stack
+};
+
 template <>
 struct WarpSmem<false> {
+    GroupConsts gc;
     int2 stack[kStackCap];
     float4 tc[32];            // (com - ref).xyz, -
     float4 tq[32];            // q = (side/theta)^2, band half-width, reach mask bits, node ref bits
-    int child[32][8];
     float4 lc[kListCap];      // (com - ref).xyz, G m
     uint32_t lm[kListCap];
     int lr[kListCap];         // node refs (adjoint mode)
@@ -72,10 +82,10 @@ struct WarpSmem<false> {
 
 template <>
 struct WarpSmem<true> {
+    GroupConsts gc;
     int2 stack[kStackCap];
     double4 tc[32];           // com.xyz (absolute), side
     int2 tr[32];              // reach mask, node ref
-    int child[32][8];
     double4 lc[kListCap];     // com.xyz (absolute), G m
     uint32_t lm[kListCap];
     int lr[kListCap];
@@ -456,10 +466,18 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
             loz = warp_minf(pz); hiz = warp_maxf(pz);
         }
 
+        if (lane == 0) {
+            s.gc.ref[0] = rx; s.gc.ref[1] = ry; s.gc.ref[2] = rz;
+            s.gc.S = S; s.gc.s_theta = s_theta;
+            s.gc.box[0] = lox; s.gc.box[1] = hix; s.gc.box[2] = loy;
+            s.gc.box[3] = hiy; s.gc.box[4] = loz; s.gc.box[5] = hiz;
+            s.gc.pm_tol = pm_tol; s.gc.tiny = tiny; s.gc.near_r2 = near_r2;
+            for (int q = 0; q < 6; q++) s.gc.st[q] = 0u;
+        }
         float fax = 0.f, fay = 0.f, faz = 0.f, fpot = 0.f;
         double dax = 0.0, day = 0.0, daz = 0.0, dpot = 0.0;
-        uint32_t cnt = 0, nint = 0, nfallback = 0, nentries = 0, ntiles = 0, ndecide = 0, nlist = 0, nnear = 0;
-        int top = 0, list_top = 0, max_top = 0;
+        uint32_t cnt = 0, nint = 0, nfallback = 0;
+        int top = 0, list_top = 0;
         uint32_t spill_top = 0;
         bool failed = false;
         if (root >= 0) {
@@ -473,11 +491,11 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
             const int cntt = min(top, 32);
             const int base = top - cntt;
             top = base;
-            nentries += cntt;
-            ntiles++;
+            if (lane == 0) { s.gc.st[0] += cntt; s.gc.st[1] += 1u; }
 
             // ---- stage: lane k takes stack entry k
             bool is_int = false;
+            int4 ch0 = make_int4(0, 0, 0, 0), ch1 = make_int4(0, 0, 0, 0);
             uint32_t reach = 0;
             int nch = 0, ref = 0;
             double cx = 0, cy = 0, cz = 0, m = 0, so = 0;
@@ -492,11 +510,8 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                     nch = meta_nchild(meta);
                     so = exp2_neg(meta_level(meta));  // 2^-level
                     const int4 *cp = reinterpret_cast<const int4 *>(t.ochild + 8 * (size_t)ref);
-                    const int4 c0 = cp[0], c1 = cp[1];
-                    s.child[lane][0] = c0.x; s.child[lane][1] = c0.y;
-                    s.child[lane][2] = c0.z; s.child[lane][3] = c0.w;
-                    s.child[lane][4] = c1.x; s.child[lane][5] = c1.y;
-                    s.child[lane][6] = c1.z; s.child[lane][7] = c1.w;
+                    ch0 = cp[0];
+                    ch1 = cp[1];
                     is_int = true;
                 } else {
                     const double4 bd = t.body[~ref];
@@ -507,7 +522,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
             }
             float fcx = 0.f, fcy = 0.f, fcz = 0.f;
             if constexpr (!kFp64) {
-                fcx = (float)(cx - rx); fcy = (float)(cy - ry); fcz = (float)(cz - rz);
+                fcx = (float)(cx - s.gc.ref[0]); fcy = (float)(cy - s.gc.ref[1]); fcz = (float)(cz - s.gc.ref[2]);
             }
 
             // ---- group-level test, one node per lane: when every point of the
@@ -519,9 +534,9 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
             bool mixed = false;
             if (is_int) {
                 if constexpr (kFp64) {
-                    const double sq = S * so / theta;
+                    const double sq = s.gc.S * so / theta;
                     const double qd = sq * sq;
-                    const double ox = cx - rx, oy = cy - ry, oz = cz - rz;
+                    const double ox = cx - s.gc.ref[0], oy = cy - s.gc.ref[1], oz = cz - s.gc.ref[2];
                     const double ax_ = fmax(fmax(dlox - ox, ox - dhix), 0.0), ay_ = fmax(fmax(dloy - oy, oy - dhiy), 0.0),
                                  az_ = fmax(fmax(dloz - oz, oz - dhiz), 0.0);
                     const double bx_ = fmax(fabs(ox - dlox), fabs(ox - dhix)), by_ = fmax(fabs(oy - dloy), fabs(oy - dhiy)),
@@ -533,16 +548,16 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                     else if (qd - r2max > tol) my_open = reach;
                     else mixed = true;
                 } else {
-                    const double sqd = s_theta * so;
+                    const double sqd = s.gc.s_theta * so;
                     const float qf = (float)(sqd * sqd), sqf = (float)sqd;
-                    const float tol = 2.f * fmaf(pm_tol, sqf, kTolRel * qf);
-                    const float ax_ = fmaxf(fmaxf(lox - fcx, fcx - hix), 0.f), ay_ = fmaxf(fmaxf(loy - fcy, fcy - hiy), 0.f),
-                                az_ = fmaxf(fmaxf(loz - fcz, fcz - hiz), 0.f);
-                    const float bx_ = fmaxf(fabsf(fcx - lox), fabsf(fcx - hix)), by_ = fmaxf(fabsf(fcy - loy), fabsf(fcy - hiy)),
-                                bz_ = fmaxf(fabsf(fcz - loz), fabsf(fcz - hiz));
+                    const float tol = 2.f * fmaf(s.gc.pm_tol, sqf, kTolRel * qf);
+                    const float ax_ = fmaxf(fmaxf(s.gc.box[0] - fcx, fcx - s.gc.box[1]), 0.f), ay_ = fmaxf(fmaxf(s.gc.box[2] - fcy, fcy - s.gc.box[3]), 0.f),
+                                az_ = fmaxf(fmaxf(s.gc.box[4] - fcz, fcz - s.gc.box[5]), 0.f);
+                    const float bx_ = fmaxf(fabsf(fcx - s.gc.box[0]), fabsf(fcx - s.gc.box[1])), by_ = fmaxf(fabsf(fcy - s.gc.box[2]), fabsf(fcy - s.gc.box[3])),
+                                bz_ = fmaxf(fabsf(fcz - s.gc.box[4]), fabsf(fcz - s.gc.box[5]));
                     const float r2min = fmaf(az_, az_, fmaf(ay_, ay_, ax_ * ax_));
                     const float r2max = fmaf(bz_, bz_, fmaf(by_, by_, bx_ * bx_));
-                    if (r2min <= 4.f * tiny) mixed = true;
+                    if (r2min <= 4.f * s.gc.tiny) mixed = true;
                     else if (r2min - qf > tol) my_open = 0;
                     else if (qf - r2max > tol) my_open = reach;
                     else mixed = true;
@@ -551,54 +566,97 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
 
             // ---- decide the mixed nodes of the tile, lane by lane
             const uint32_t intm = __ballot_sync(FULL, mixed);
-            ndecide += __popc(intm);
+            if (lane == 0) s.gc.st[2] += __popc(intm);
             if (intm) {
                 if constexpr (kFp64) {
-                    s.tc[lane] = make_double4(cx, cy, cz, S * so);
+                    s.tc[lane] = make_double4(cx, cy, cz, s.gc.S * so);
                     s.tr[lane] = make_int2((int)reach, ref);
                 } else {
-                    const double sq = s_theta * so;
+                    const double sq = s.gc.s_theta * so;
                     const float qf = (float)(sq * sq);
                     s.tc[lane] = make_float4(fcx, fcy, fcz, 0.f);
-                    s.tq[lane] = make_float4(qf, fmaf(pm_tol, (float)sq, kTolRel * qf), __uint_as_float(reach),
+                    s.tq[lane] = make_float4(qf, fmaf(s.gc.pm_tol, (float)sq, kTolRel * qf), __uint_as_float(reach),
                                              __int_as_float(ref));
                 }
                 __syncwarp();
                 uint32_t mm = intm;
-                while (mm) {
-                    const int k = __ffs(mm) - 1;
-                    mm &= mm - 1;
-                    bool open;
-                    uint32_t rk;
-                    if constexpr (kFp64) {
-                        const double4 c = s.tc[k];
-                        const int2 tr = s.tr[k];
-                        rk = (uint32_t)tr.x;
-                        const double dx = __dsub_rn(c.x, b.x), dy = __dsub_rn(c.y, b.y), dz = __dsub_rn(c.z, b.z);
-                        const double d = __dsqrt_rn(
-                            __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
-                        open = __ddiv_rn(c.w, d) > theta;
-                    } else {
-                        const float4 c = s.tc[k];
-                        const float4 q = s.tq[k];
-                        rk = __float_as_uint(q.z);
-                        const float dx = c.x - px, dy = c.y - py, dz = c.z - pz;
-                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                        const float d = r2 - q.x;
-                        open = d < 0.f;
-                        const bool amb = ((rk >> lane) & 1u) && (fabsf(d) <= q.y || r2 <= tiny);
-                        if (__any_sync(FULL, amb)) {
-                            if (amb) {
-                                const int node = __float_as_int(q.w);
+                if constexpr (kFp64) {
+                    uint32_t mm = intm;
+                    while (mm) {
+                        const int k = __ffs(mm) - 1;
+                        mm &= mm - 1;
+                        bool open;
+                        uint32_t rk;
+                        if constexpr (kFp64) {
+                            const double4 c = s.tc[k];
+                            const int2 tr = s.tr[k];
+                            rk = (uint32_t)tr.x;
+                            const double dx = __dsub_rn(c.x, b.x), dy = __dsub_rn(c.y, b.y), dz = __dsub_rn(c.z, b.z);
+                            const double d = __dsqrt_rn(
+                                __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+                            open = __ddiv_rn(c.w, d) > theta;
+                        } else {
+                            const float4 c = s.tc[k];
+                            const float4 q = s.tq[k];
+                            rk = __float_as_uint(q.z);
+                            const float dx = c.x - px, dy = c.y - py, dz = c.z - pz;
+                            const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                            const float d = r2 - q.x;
+                            open = d < 0.f;
+                            const bool amb = ((rk >> lane) & 1u) && (fabsf(d) <= q.y || r2 <= s.gc.tiny);
+                            if (__any_sync(FULL, amb)) {
+                                if (amb) {
+                                    const int node = __float_as_int(q.w);
+                                    const double4 nd = t.onode[node];
+                                    const double side = s.gc.S * exp2_neg(meta_level(t.ometa[node]));
+                                    open = exact_open(nd.x, nd.y, nd.z, b.x, b.y, b.z, side, theta);
+                                    nfallback++;
+                                }
+                            }
+                        }
+                        const uint32_t om = __ballot_sync(FULL, open) & rk;
+                        if (lane == k) my_open = om;
+                    }
+                } else {
+                    // two mixed nodes per round: their tests are independent
+                    const float tiny_ = s.gc.tiny;
+                    while (mm) {
+                        const int k1 = __ffs(mm) - 1;
+                        mm &= mm - 1;
+                        const int k2 = mm ? __ffs(mm) - 1 : k1;
+                        if (mm) mm &= mm - 1;
+                        const float4 c1 = s.tc[k1], q1 = s.tq[k1];
+                        const float4 c2 = s.tc[k2], q2 = s.tq[k2];
+                        const uint32_t rk1 = __float_as_uint(q1.z), rk2 = __float_as_uint(q2.z);
+                        const float dx1 = c1.x - px, dy1 = c1.y - py, dz1 = c1.z - pz;
+                        const float dx2 = c2.x - px, dy2 = c2.y - py, dz2 = c2.z - pz;
+                        const float r21 = fmaf(dz1, dz1, fmaf(dy1, dy1, dx1 * dx1));
+                        const float r22 = fmaf(dz2, dz2, fmaf(dy2, dy2, dx2 * dx2));
+                        const float d1 = r21 - q1.x, d2 = r22 - q2.x;
+                        bool open1 = d1 < 0.f, open2 = d2 < 0.f;
+                        const bool amb1 = ((rk1 >> lane) & 1u) && (fabsf(d1) <= q1.y || r21 <= tiny_);
+                        const bool amb2 = k2 != k1 && ((rk2 >> lane) & 1u) && (fabsf(d2) <= q2.y || r22 <= tiny_);
+                        if (__any_sync(FULL, amb1 || amb2)) {
+                            if (amb1) {
+                                const int node = __float_as_int(q1.w);
                                 const double4 nd = t.onode[node];
-                                const double side = S * exp2_neg(meta_level(t.ometa[node]));
-                                open = exact_open(nd.x, nd.y, nd.z, b.x, b.y, b.z, side, theta);
+                                const double side = s.gc.S * exp2_neg(meta_level(t.ometa[node]));
+                                open1 = exact_open(nd.x, nd.y, nd.z, b.x, b.y, b.z, side, theta);
+                                nfallback++;
+                            }
+                            if (amb2) {
+                                const int node = __float_as_int(q2.w);
+                                const double4 nd = t.onode[node];
+                                const double side = s.gc.S * exp2_neg(meta_level(t.ometa[node]));
+                                open2 = exact_open(nd.x, nd.y, nd.z, b.x, b.y, b.z, side, theta);
                                 nfallback++;
                             }
                         }
+                        const uint32_t om1 = __ballot_sync(FULL, open1) & rk1;
+                        const uint32_t om2 = __ballot_sync(FULL, open2) & rk2;
+                        if (lane == k1) my_open = om1;
+                        if (k2 != k1 && lane == k2) my_open = om2;
                     }
-                    const uint32_t om = __ballot_sync(FULL, open) & rk;
-                    if (lane == k) my_open = om;
                 }
             }
 
@@ -611,9 +669,9 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
             bool near = false;
             if constexpr (!kFp64) {
                 if (accm) {
-                    const float ax_ = fmaxf(fmaxf(lox - fcx, fcx - hix), 0.f), ay_ = fmaxf(fmaxf(loy - fcy, fcy - hiy), 0.f),
-                                az_ = fmaxf(fmaxf(loz - fcz, fcz - hiz), 0.f);
-                    near = fmaf(az_, az_, fmaf(ay_, ay_, ax_ * ax_)) < near_r2;
+                    const float ax_ = fmaxf(fmaxf(s.gc.box[0] - fcx, fcx - s.gc.box[1]), 0.f), ay_ = fmaxf(fmaxf(s.gc.box[2] - fcy, fcy - s.gc.box[3]), 0.f),
+                                az_ = fmaxf(fmaxf(s.gc.box[4] - fcz, fcz - s.gc.box[5]), 0.f);
+                    near = fmaf(az_, az_, fmaf(ay_, ay_, ax_ * ax_)) < s.gc.near_r2;
                 }
             }
             const uint32_t am = __ballot_sync(FULL, accm != 0 && !near);
@@ -625,7 +683,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                 s.lr[pos] = ref;
             }
             list_top += __popc(am);
-            nlist += __popc(am);
+            if (lane == 0) s.gc.st[3] += __popc(am);
             if constexpr (!kFp64) {
                 const uint32_t nmk = __ballot_sync(FULL, near);
                 if (nmk) {
@@ -642,20 +700,18 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                     else
                         force_near_f32<kDamp, kPot>(s.nc, s.nm, __popc(nmk), lane, b.x, b.y, b.z, fax, fay, faz, fpot);
                     if (a.counts) cnt += count_list(s.nm, __popc(nmk), 1u << lane);
-                    nnear += __popc(nmk);
+                    if (lane == 0) s.gc.st[4] += __popc(nmk);
                     __syncwarp();
                 }
             }
 
             // ---- children of opened nodes -> stack
+            // exclusive prefix of the child counts (0..8) from four independent ballots of their bits
             const int myn = my_open ? nch : 0;
-            int pre = myn;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(FULL, pre, o);
-                if (lane >= o) pre += y;
-            }
-            const int total = __shfl_sync(FULL, pre, 31);
-            pre -= myn;
+            const uint32_t q0 = __ballot_sync(FULL, myn & 1), q1 = __ballot_sync(FULL, myn & 2),
+                           q2 = __ballot_sync(FULL, myn & 4), q3 = __ballot_sync(FULL, myn & 8);
+            const int pre = __popc(q0 & lt) + 2 * __popc(q1 & lt) + 4 * __popc(q2 & lt) + 8 * __popc(q3 & lt);
+            const int total = __popc(q0) + 2 * __popc(q1) + 4 * __popc(q2) + 8 * __popc(q3);
             if (total > 0) {
                 if (top + total > kStackCap) {
                     if (!spill_out(s, top, spill_top, gspill, a.spill_cap, lane)) {
@@ -663,9 +719,18 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                         break;
                     }
                 }
-                for (int i = 0; i < myn; i++) s.stack[top + pre + i] = make_int2(s.child[lane][i], (int)my_open);
+                int2 *dst = s.stack + top + pre;
+                const int om = (int)my_open;
+                if (myn > 0) dst[0] = make_int2(ch0.x, om);
+                if (myn > 1) dst[1] = make_int2(ch0.y, om);
+                if (myn > 2) dst[2] = make_int2(ch0.z, om);
+                if (myn > 3) dst[3] = make_int2(ch0.w, om);
+                if (myn > 4) dst[4] = make_int2(ch1.x, om);
+                if (myn > 5) dst[5] = make_int2(ch1.y, om);
+                if (myn > 6) dst[6] = make_int2(ch1.z, om);
+                if (myn > 7) dst[7] = make_int2(ch1.w, om);
                 top += total;
-                max_top = max(max_top, top + (int)spill_top);
+                if (lane == 0) s.gc.st[5] = max(s.gc.st[5], (uint32_t)(top + (int)spill_top));
             }
             __syncwarp();
 
@@ -716,12 +781,12 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
             atomicAdd(&t.sc->interactions, wc);
             atomicAdd(&t.sc->interactions_total, wc);
             if (wf) atomicAdd(&t.sc->fallback_tests, wf);
-            atomicAdd(&t.sc->walk_entries, (unsigned long long)nentries);
-            atomicAdd(&t.sc->walk_tiles, (unsigned long long)ntiles);
-            atomicAdd(&t.sc->walk_decisions, (unsigned long long)ndecide);
-            atomicAdd(&t.sc->walk_list, (unsigned long long)nlist);
-            if (nnear) atomicAdd(&t.sc->walk_near, (unsigned long long)nnear);
-            atomicMax(&t.sc->max_stack, (uint32_t)max_top);
+            atomicAdd(&t.sc->walk_entries, (unsigned long long)s.gc.st[0]);
+            atomicAdd(&t.sc->walk_tiles, (unsigned long long)s.gc.st[1]);
+            atomicAdd(&t.sc->walk_decisions, (unsigned long long)s.gc.st[2]);
+            atomicAdd(&t.sc->walk_list, (unsigned long long)s.gc.st[3]);
+            if (s.gc.st[4]) atomicAdd(&t.sc->walk_near, (unsigned long long)s.gc.st[4]);
+            atomicMax(&t.sc->max_stack, s.gc.st[5]);
             if (!kAdj && a.track_max_acc) atomic_max_nonneg(&t.sc->max_acc_bits, amag);
         }
     }
@@ -745,6 +810,9 @@ const void *any_walk_kernel(bool fp64, bool adj, int damping, bool pot) {
 
 }  // namespace
 
+constexpr size_t kLargestWarpSmem =
+    sizeof(WarpSmem<true>) > sizeof(WarpSmem<false>) ? sizeof(WarpSmem<true>) : sizeof(WarpSmem<false>);
+
 cudaError_t walk_max_blocks_per_sm(bool fp64, unsigned warps, int *out) {
     const size_t smem = (fp64 ? sizeof(WarpSmem<true>) : sizeof(WarpSmem<false>)) * warps;
     int minblocks = 1 << 30;
@@ -753,7 +821,7 @@ cudaError_t walk_max_blocks_per_sm(bool fp64, unsigned warps, int *out) {
             for (int pot = 0; pot < 2 - adj; pot++) {
                 const void *k = any_walk_kernel(fp64, adj, damp, pot);
                 cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     (int)(sizeof(WarpSmem<true>) * kWalkMaxWarps));
+                                                     (int)(kLargestWarpSmem * kWalkMaxWarps));
                 if (e != cudaSuccess) return e;
                 int nb = 0;
                 e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, (int)warps * 32, smem);

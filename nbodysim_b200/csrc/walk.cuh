@@ -7,7 +7,7 @@ namespace nbody {
 
 constexpr int kWalkWarps = 4;       // default warps per block (the autotuner may pick 1 or 2)
 constexpr int kWalkMaxWarps = 4;    // largest block the walk kernel is compiled for
-constexpr int kStackCap = 768;      // shared-memory stack entries per warp
+constexpr int kStackCap = 640;      // shared-memory stack entries per warp
 constexpr int kSpillChunk = kStackCap / 2;
 constexpr int kListFlush = 32;      // force pass once the interaction list holds this many
 constexpr int kListCap = kListFlush + 32;
