@@ -85,6 +85,11 @@ struct nbody_ctx {
     size_t adj_bytes = 0;
     double *lx = nullptr, *lv = nullptr, *lm = nullptr, *lam = nullptr, *gdir = nullptr;
     double *adj_node = nullptr, *adj_leaf = nullptr, *vel_work = nullptr, *seg_pos = nullptr, *ckpt = nullptr;
+    // Octrees of one checkpoint segment, kept by the recomputation so that the
+    // reverse pass at the same positions does not rebuild them (single system;
+    // left out when the memory is not there).
+    double *tree_slots = nullptr;
+    uint32_t n_slots = 0;
     uint32_t fwd_steps = 0, fwd_every = 0, fwd_n = 0;
     double fwd_dt = 0.0;
     bool have_fwd = false;
@@ -254,10 +259,11 @@ void ev(nbody_ctx *c, int k) {
 
 // One force pass on the resident pos/mass: tree, COM, walk. Asynchronous.
 int apply_min_size(nbody_ctx *c, bool want_vmax, unsigned *launches);
+int copy_tree_slot(nbody_ctx *c, uint32_t i, bool save);
 
 int force_pass(nbody_ctx *c, int damping, double theta, bool fp64, bool want_vmax, bool track_amax,
                bool want_counts, bool want_pot, const double *pos = nullptr, bool adjoint = false,
-               const WalkLaunch *shape = nullptr, bool min_size = false) {
+               const WalkLaunch *shape = nullptr, bool min_size = false, int save_slot = -1, int restore_slot = -1) {
     uint32_t n = c->n;
     unsigned launches = 1;
     NB_CUDA(launch_reset_pass(c->sc, c->stream));
@@ -271,14 +277,25 @@ int force_pass(nbody_ctx *c, int damping, double theta, bool fp64, bool want_vma
     c->tb.sys_root = c->sys_root;
     c->tb.sys_root_node = c->sys_root_node;
     ev(c, 0);
-    NB_CUDA(build_octree(c->tb, c->stream, &launches));
-    if (min_size && c->p.min_node_size > 0 && n >= 2 && !multi) {
-        int rc = apply_min_size(c, want_vmax, &launches);
+    if (restore_slot >= 0 && !multi) {
+        // the octree of these positions was saved by the forward recomputation
+        int rc = copy_tree_slot(c, (uint32_t)restore_slot, false);
         if (rc) return rc;
-        n = c->n;
+        ev(c, 1);
+    } else {
+        NB_CUDA(build_octree(c->tb, c->stream, &launches));
+        if (min_size && c->p.min_node_size > 0 && n >= 2 && !multi) {
+            int rc = apply_min_size(c, want_vmax, &launches);
+            if (rc) return rc;
+            n = c->n;
+        }
+        ev(c, 1);
+        NB_CUDA(compute_com(c->tb, c->stream, &launches));
+        if (save_slot >= 0 && !multi) {
+            int rc = copy_tree_slot(c, (uint32_t)save_slot, true);
+            if (rc) return rc;
+        }
     }
-    ev(c, 1);
-    NB_CUDA(compute_com(c->tb, c->stream, &launches));
     ev(c, 2);
     WalkArgs a{};
     a.t.n = n;
@@ -621,7 +638,57 @@ int run_steps(nbody_ctx *c, uint32_t nsteps) {
 
 // Adjoint buffers for n particles, `seg` positions per checkpoint segment and
 // `nckpt` checkpoints of (pos, vel).
-int reserve_adjoint(nbody_ctx *c, uint32_t n, uint32_t seg, uint32_t nckpt) {
+// Bytes of one saved octree of n particles (tree_slot_ptrs below).
+size_t tree_slot_bytes(uint32_t n) {
+    const size_t N = n;
+    return align256(32 * N) + align256(4 * N) + align256(32 * N) + align256(32 * N) + align256(4 * N) +
+           align256(4 * N) + align256(4 * N) + align256(32);
+}
+
+struct TreeSlot {
+    double4 *body, *onode;
+    uint32_t *sidx;
+    int32_t *ochild, *ometa, *oparent, *leaf_oparent;
+    double *root;  // root_center[3], root_side
+};
+
+TreeSlot tree_slot_ptrs(nbody_ctx *c, uint32_t i) {
+    const size_t N = c->n;
+    char *p = (char *)c->tree_slots + tree_slot_bytes(c->n) * i;
+    TreeSlot t;
+    t.body = (double4 *)p; p += align256(32 * N);
+    t.sidx = (uint32_t *)p; p += align256(4 * N);
+    t.onode = (double4 *)p; p += align256(32 * N);
+    t.ochild = (int32_t *)p; p += align256(32 * N);
+    t.ometa = (int32_t *)p; p += align256(4 * N);
+    t.oparent = (int32_t *)p; p += align256(4 * N);
+    t.leaf_oparent = (int32_t *)p; p += align256(4 * N);
+    t.root = (double *)p;
+    return t;
+}
+
+// Copies the octree just built to slot i (save) or slot i to the build buffers.
+int copy_tree_slot(nbody_ctx *c, uint32_t i, bool save) {
+    const size_t N = c->n, M = N > 0 ? N - 1 : 0;
+    const TreeSlot t = tree_slot_ptrs(c, i);
+    TreeBuild &tb = c->tb;
+    struct Pair { void *slot; void *live; size_t bytes; } pairs[] = {
+        {t.body, tb.body, 32 * N}, {t.sidx, tb.idx_a, 4 * N}, {t.onode, tb.onode, 32 * M},
+        {t.ochild, tb.ochild, 32 * M}, {t.ometa, tb.ometa, 4 * M}, {t.oparent, tb.oparent, 4 * M},
+        {t.leaf_oparent, tb.leaf_oparent, 4 * N}, {t.root, c->sc->root_center, 32},
+    };
+    for (auto &q : pairs) {
+        if (!q.bytes) continue;
+        NB_CUDA(cudaMemcpyAsync(save ? q.slot : q.live, save ? q.live : q.slot, q.bytes, cudaMemcpyDeviceToDevice,
+                                c->stream));
+    }
+    return NBODY_OK;
+}
+
+// Adjoint buffers for n particles, `seg` positions per checkpoint segment and
+// `nckpt` checkpoints of (pos, vel); with `slots`, room for `seg` saved octrees
+// as well when the device has it.
+int reserve_adjoint(nbody_ctx *c, uint32_t n, uint32_t seg, uint32_t nckpt, bool slots = false) {
     const size_t N = n;
     struct Piece { double **dst; size_t bytes; };
     Piece pieces[] = {
@@ -631,23 +698,42 @@ int reserve_adjoint(nbody_ctx *c, uint32_t n, uint32_t seg, uint32_t nckpt) {
     };
     size_t total = 0;
     for (auto &pc : pieces) total += align256(pc.bytes);
-    if (total > c->adj_bytes) {
+    size_t with_slots = total;
+    if (slots && c->nsys <= 1) {
+        size_t free_b = 0, tot_b = 0;
+        if (cudaMemGetInfo(&free_b, &tot_b) != cudaSuccess) cudaGetLastError();
+        const size_t extra = tree_slot_bytes(n) * seg;
+        // keep a margin: the slots are an optimisation, never worth an allocation failure
+        if (extra + total < c->adj_bytes || extra + total < free_b / 2) with_slots = total + extra;
+    }
+    if (with_slots > c->adj_bytes) {
         NB_CUDA(cudaStreamSynchronize(c->stream));
         if (c->adj_arena) NB_CUDA(cudaFree(c->adj_arena));
         c->adj_arena = nullptr;
         c->adj_bytes = 0;
-        cudaError_t e = cudaMalloc(&c->adj_arena, total);
+        cudaError_t e = cudaMalloc(&c->adj_arena, with_slots);
+        if (e != cudaSuccess && with_slots > total) {
+            cudaGetLastError();
+            with_slots = total;
+            e = cudaMalloc(&c->adj_arena, total);
+        }
         if (e != cudaSuccess) {
             cudaGetLastError();
             c->adj_arena = nullptr;
             return fail(NBODY_ERR_OOM, "adjoint buffers (%s)", cudaGetErrorString(e));
         }
-        c->adj_bytes = total;
+        c->adj_bytes = with_slots;
     }
     char *p = (char *)c->adj_arena;
     for (auto &pc : pieces) {
         *pc.dst = (double *)p;
         p += align256(pc.bytes);
+    }
+    c->tree_slots = nullptr;
+    c->n_slots = 0;
+    if (with_slots > total) {
+        c->tree_slots = (double *)p;
+        c->n_slots = seg;
     }
     return NBODY_OK;
 }
@@ -655,8 +741,8 @@ int reserve_adjoint(nbody_ctx *c, uint32_t n, uint32_t seg, uint32_t nckpt) {
 // One reverse force step at positions `pos` with cotangent c->lam (dL/da):
 // tree and COM at pos, the adjoint walk over the same decisions, then the node
 // cotangents distributed to particles; adds into c->lx and c->lm.
-int adjoint_force(nbody_ctx *c, const double *pos, int damping, double theta, bool fp64) {
-    int rc = force_pass(c, damping, theta, fp64, false, false, false, false, pos, true);
+int adjoint_force(nbody_ctx *c, const double *pos, int damping, double theta, bool fp64, int restore_slot = -1) {
+    int rc = force_pass(c, damping, theta, fp64, false, false, false, false, pos, true, nullptr, false, -1, restore_slot);
     if (rc) return rc;
     NB_CUDA(launch_adj_distribute(c->tb.body, c->tb.idx_a, c->tb.leaf_oparent, c->tb.oparent, c->tb.onode,
                                   c->adj_node, c->adj_leaf, c->gdir, fp64, c->lx, c->lm, c->n, c->stream));
@@ -1144,6 +1230,7 @@ int nbody_force_vjp(nbody_ctx *c, uint32_t n, const double *pos, const double *m
     if (n == 0) return NBODY_OK;
     int rc = upload(c, n, pos, nullptr, mass);
     if (rc) return rc;
+    c->have_fwd = false;  // the state and the adjoint buffers are reused here
     if ((rc = reserve_adjoint(c, n, 1, 0))) return rc;
     if ((rc = begin_call(c))) return rc;
     const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
@@ -1176,7 +1263,7 @@ int nbody_forward_checkpointed(nbody_ctx *c, uint32_t nsteps, uint32_t every) {
     }
     if (every > nsteps) every = nsteps;
     const uint32_t nseg = (nsteps + every - 1) / every;
-    int rc = reserve_adjoint(c, c->n, every, nseg);
+    int rc = reserve_adjoint(c, c->n, every, nseg, true);
     if (rc) return rc;
     if ((rc = begin_call(c))) return rc;
     if ((rc = maybe_autotune(c))) return rc;
@@ -1236,7 +1323,9 @@ int nbody_backward(nbody_ctx *c, const double *dL_dpos, const double *dL_dvel, d
                 double *xi = c->seg_pos + N3 * i, *xn = xi + N3;
                 NB_CUDA(cudaMemcpyAsync(xn, xi, 8 * N3, cudaMemcpyDeviceToDevice, c->stream));
                 // forces at xi, then update the copy in place: x_{k+1}, v_{k+1}
-                int r = force_pass(c, c->p.damping, c->p.theta, fp64, false, false, false, false, xi, false);
+                const int save = i < c->n_slots ? (int)i : -1;
+                int r = force_pass(c, c->p.damping, c->p.theta, fp64, false, false, false, false, xi, false, nullptr,
+                                   false, save, -1);
                 if (r) return r;
                 StepParams sp{c->p.dt, 0, 0, 0, 0};
                 NB_CUDA(launch_update(xn, c->vel_work, c->acc, fp64, n, sp, c->sc, c->stream));
@@ -1249,7 +1338,9 @@ int nbody_backward(nbody_ctx *c, const double *dL_dpos, const double *dL_dvel, d
             auto adj = [&, i]() -> int {
                 NB_CUDA(launch_adj_pre(c->lx, c->lv, c->lam, fp64, c->p.dt, n, c->stream));
                 c->launches++;
-                return adjoint_force(c, c->seg_pos + N3 * (size_t)i, c->p.damping, c->p.theta, fp64);
+                // positions 0 .. len-2 of the segment had their octrees saved by the recomputation
+                const int restore = (uint32_t)i + 1 < len && (uint32_t)i < c->n_slots ? i : -1;
+                return adjoint_force(c, c->seg_pos + N3 * (size_t)i, c->p.damping, c->p.theta, fp64, restore);
             };
             if ((rc = run_cached(c, c->adj_exec, c->adj_launches, (uint32_t)i, adj))) return rc;
         }
