@@ -1142,12 +1142,14 @@ int nbody_step_host(nbody_ctx *c, uint32_t n, double *pos, double *vel, const do
             NB_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
             NB_CUDA(cudaEventCreateWithFlags(&c->ev_vel, cudaEventDisableTiming));
         }
+        // The velocity copy starts once the positions and masses are in, so that it
+        // does not share the host link with them.
+        NB_CUDA(cudaMemcpyAsync(c->pos, pos, 24 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+        NB_CUDA(cudaMemcpyAsync(c->mass, mass, 8 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
         NB_CUDA(cudaEventRecord(c->ev_fork, c->stream));
         NB_CUDA(cudaStreamWaitEvent(c->aux_stream, c->ev_fork, 0));
         NB_CUDA(cudaMemcpyAsync(c->vel, vel, 24 * (size_t)n, cudaMemcpyHostToDevice, c->aux_stream));
         NB_CUDA(cudaEventRecord(c->ev_vel, c->aux_stream));
-        NB_CUDA(cudaMemcpyAsync(c->pos, pos, 24 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
-        NB_CUDA(cudaMemcpyAsync(c->mass, mass, 8 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
         c->n = n;
         c->have_state = c->have_vel = true;
         c->have_acc = false;
