@@ -498,12 +498,12 @@ __global__ void k_com(const double4 *__restrict__ body, const int32_t *__restric
         }
         const int32_t meta = ometa[p];
         const int nch = meta_nchild(meta);
-        // Release: a thread that wrote a node (hops > 0) makes it visible
-        // before counting itself in; a leaf thread has written nothing.
-        if (hops > 0) __threadfence();
-        uint32_t old = atomicAdd(&ocount[p], 1u);
+        // One acquire-release count: it publishes the node this thread wrote on
+        // the previous hop, and the last child to arrive sees every other
+        // child's result.
+        uint32_t old;
+        asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(&ocount[p]) : "memory");
         if (old != (uint32_t)(nch - 1)) return;
-        __threadfence();  // acquire: the other children's results are visible
         // The reference sums the masses, then the mass-weighted centres, each in
         // child order; both sums run here in one pass over the children.
         const int L = meta_level(meta);
