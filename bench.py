@@ -291,7 +291,9 @@ def run_ours(args) -> None:
             pg.destroy_process_group()
         return
 
-    # ---- the plain FP64 form on the same workload, same initial state, same K
+    # ---- the plain FP64 form on the same workload, same initial state, same K.
+    # This and the legs below are single-GPU comparisons: under torchrun only the
+    # headline runs, so rank 0 does not keep the other ranks waiting at the barrier.
     fp64_ms_step = None
     with nb.Engine(nb.default_params(theta=args.theta, adaptive=1, min_adaptive_dt=0.00333, max_pos_change=3.0,
                                      max_vel_change=3.0, precision=nb.PRECISION_FP64, device=local)) as e64:
@@ -308,17 +310,17 @@ def run_ours(args) -> None:
 
     # ---- adjoint / forward at the adjoint configuration (sphere N=65536, K=256, checkpoint 16)
     adjoint = None
-    if not args.no_adjoint:
+    if not args.no_adjoint and world == 1:
         adjoint = adjoint_leg(nb, torch, stream, local, args.adjoint_fd)
 
     # ---- batched ensemble (512 systems of uneven N, one persistent walk, graphs, autotuned)
     ensemble = None
-    if not args.no_ensemble:
+    if not args.no_ensemble and world == 1:
         ensemble = ensemble_leg(nb, torch, stream, local)
 
     # ---- the other configurations: cube 5000 x 300 frames, sphere 100k x 100 steps, theta sweep at 1M
     configs = None
-    if not args.no_configs:
+    if not args.no_configs and world == 1:
         configs = {"cube5000": cube_leg(nb, torch, stream, local),
                    "sphere100k": sphere_leg(nb, torch, stream, local),
                    "shell1M_theta": theta_leg(nb, torch, stream, local, pos0, vel0, mass)}
