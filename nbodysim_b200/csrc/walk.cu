@@ -145,7 +145,7 @@ __device__ inline void force_list_f32(const float4 *lc, const uint32_t *lm, int 
                                       float py, float pz, float &ax, float &ay, float &az, float &pot) {
     float bx = 0.f, by = 0.f, bz = 0.f, bp = 0.f;
     int k = 0;
-#pragma unroll 2
+#pragma unroll 4
     for (; k + 1 < count; k += 2) {
         const float4 c0 = lc[k], c1 = lc[k + 1];
         const uint32_t m0 = lm[k], m1 = lm[k + 1];
