@@ -581,39 +581,16 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                 __syncwarp();
                 uint32_t mm = intm;
                 if constexpr (kFp64) {
-                    uint32_t mm = intm;
+                    // the FP64 form decides every mixed node with the reference's own test
                     while (mm) {
                         const int k = __ffs(mm) - 1;
                         mm &= mm - 1;
-                        bool open;
-                        uint32_t rk;
-                        if constexpr (kFp64) {
-                            const double4 c = s.tc[k];
-                            const int2 tr = s.tr[k];
-                            rk = (uint32_t)tr.x;
-                            const double dx = __dsub_rn(c.x, b.x), dy = __dsub_rn(c.y, b.y), dz = __dsub_rn(c.z, b.z);
-                            const double d = __dsqrt_rn(
-                                __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
-                            open = __ddiv_rn(c.w, d) > theta;
-                        } else {
-                            const float4 c = s.tc[k];
-                            const float4 q = s.tq[k];
-                            rk = __float_as_uint(q.z);
-                            const float dx = c.x - px, dy = c.y - py, dz = c.z - pz;
-                            const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                            const float d = r2 - q.x;
-                            open = d < 0.f;
-                            const bool amb = ((rk >> lane) & 1u) && (fabsf(d) <= q.y || r2 <= s.gc.tiny);
-                            if (__any_sync(FULL, amb)) {
-                                if (amb) {
-                                    const int node = __float_as_int(q.w);
-                                    const double4 nd = t.onode[node];
-                                    const double side = s.gc.S * exp2_neg(meta_level(t.ometa[node]));
-                                    open = exact_open(nd.x, nd.y, nd.z, b.x, b.y, b.z, side, theta);
-                                    nfallback++;
-                                }
-                            }
-                        }
+                        const double4 c = s.tc[k];
+                        const uint32_t rk = (uint32_t)s.tr[k].x;
+                        const double dx = __dsub_rn(c.x, b.x), dy = __dsub_rn(c.y, b.y), dz = __dsub_rn(c.z, b.z);
+                        const double d = __dsqrt_rn(
+                            __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+                        const bool open = __ddiv_rn(c.w, d) > theta;
                         const uint32_t om = __ballot_sync(FULL, open) & rk;
                         if (lane == k) my_open = om;
                     }
