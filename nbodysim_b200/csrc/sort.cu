@@ -7,7 +7,8 @@
 // publishes its per-digit count, adds the counts of all earlier tiles by
 // decoupled look-back (a tile only ever waits for tiles that started before
 // it, so the wait always ends; it is still bounded, and a timeout is reported
-// as an error), and scatters.
+// as an error), and scatters: the tile is first laid out in digit order in
+// shared memory, so that each digit's run goes out in coalesced writes.
 #include "sort.cuh"
 
 namespace nbody {
@@ -71,6 +72,9 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint64_t *__restric
                                                        uint32_t *ticket, uint32_t *err, uint32_t err_bit) {
     __shared__ uint32_t s_wc[kWarps][256];  // per-warp digit counts, then per-warp offsets
     __shared__ uint32_t s_base[256];        // global position of the tile's first key of each digit
+    __shared__ uint32_t s_lstart[256];      // position of each digit's first key within the tile
+    __shared__ uint32_t s_wsum[kWarps];
+    __shared__ uint64_t s_buf[kTile];       // the tile in digit order: keys, then indices
     __shared__ uint32_t s_tile;
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     if (t == 0) s_tile = atomicAdd(ticket, 1u);
@@ -104,6 +108,20 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint64_t *__restric
         const uint32_t c = s_wc[k][t];
         s_wc[k][t] = total;
         total += c;
+    }
+    // ---- tile-local start of each digit (exclusive scan of the 256 totals)
+    {
+        uint32_t x = total;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) s_wsum[w] = x;
+        __syncthreads();
+        uint32_t off = 0;
+        for (int k = 0; k < w; k++) off += s_wsum[k];
+        s_lstart[t] = off + x - total;
     }
     // ---- decoupled look-back over earlier tiles
     uint32_t *st = status + (size_t)tile * 256 + t;
@@ -142,16 +160,45 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint64_t *__restric
     }
     s_base[t] = goff[t] + excl;
     __syncthreads();
-    // ---- scatter
+    // ---- scatter through shared memory: the tile is laid out in digit order,
+    // then consecutive threads write consecutive positions of each digit's run
+    const uint32_t tcount = min(kTile, n - tile * kTile);
 #pragma unroll
     for (int r = 0; r < kItems; r++) {
         const uint32_t i = base + r * 32 + lane;
         if (i < n) {
             const uint32_t d = (uint32_t)((key[r] >> shift) & 255u);
-            const uint32_t pos = s_base[d] + s_wc[w][d] + rank[r];
-            kout[pos] = key[r];
-            iout[pos] = idx[r];
+            s_buf[s_lstart[d] + s_wc[w][d] + rank[r]] = key[r];
         }
+    }
+    __syncthreads();
+    uint32_t dslot[kItems];
+#pragma unroll
+    for (int r = 0; r < kItems; r++) {
+        const uint32_t q = (uint32_t)t + r * kThreads;
+        dslot[r] = 0;
+        if (q < tcount) {
+            const uint64_t k = s_buf[q];
+            const uint32_t d = (uint32_t)((k >> shift) & 255u);
+            dslot[r] = d;
+            kout[s_base[d] + (q - s_lstart[d])] = k;
+        }
+    }
+    __syncthreads();
+    uint32_t *s_idx = reinterpret_cast<uint32_t *>(s_buf);
+#pragma unroll
+    for (int r = 0; r < kItems; r++) {
+        const uint32_t i = base + r * 32 + lane;
+        if (i < n) {
+            const uint32_t d = (uint32_t)((key[r] >> shift) & 255u);
+            s_idx[s_lstart[d] + s_wc[w][d] + rank[r]] = idx[r];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kItems; r++) {
+        const uint32_t q = (uint32_t)t + r * kThreads;
+        if (q < tcount) iout[s_base[dslot[r]] + (q - s_lstart[dslot[r]])] = s_idx[q];
     }
 }
 
