@@ -657,7 +657,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                 if constexpr (kFp64) s.lc[pos] = make_double4(cx, cy, cz, kG * m);
                 else s.lc[pos] = make_float4(fcx, fcy, fcz, (float)(kG * m));
                 s.lm[pos] = accm;
-                s.lr[pos] = ref;
+                if constexpr (kAdj) s.lr[pos] = ref;
             }
             list_top += __popc(am);
             if (lane == 0) s.gc.st[3] += __popc(am);
@@ -668,7 +668,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                         const int pos = __popc(nmk & lt);
                         s.nc[pos] = make_double4(cx, cy, cz, kG * m);
                         s.nm[pos] = accm;
-                        s.nr[pos] = ref;
+                        if constexpr (kAdj) s.nr[pos] = ref;
                     }
                     __syncwarp();
                     if constexpr (kAdj)
