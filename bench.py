@@ -14,7 +14,8 @@ cube -> Morton keys -> radix sort -> octree -> mass/COM -> fused walk + gravity
   roofline     the fused walk kernel: 20 FLOP per interaction (the customary
                N-body count) against the measured FP32 FMA peak
   cpu_baseline the reference's own CPU walk (oracle/_ref, all host threads) on a
-               bounded sample of the same workload
+               bounded sample of the same workload; also the reference's frame
+               loop on config 1, which checks the GPU's final positions
 
 `--impl reference` times the reference's CPU implementation alone (rank 0).
 """
@@ -321,7 +322,8 @@ def run_ours(args) -> None:
     # ---- the other configurations: cube 5000 x 300 frames, sphere 100k x 100 steps, theta sweep at 1M
     configs = None
     if not args.no_configs and world == 1:
-        configs = {"cube5000": cube_leg(nb, torch, stream, local),
+        cube, cube_inputs = cube_leg(nb, torch, stream, local)
+        configs = {"cube5000": cube,
                    "sphere100k": sphere_leg(nb, torch, stream, local),
                    "shell1M_theta": theta_leg(nb, torch, stream, local, pos0, vel0, mass)}
 
@@ -338,16 +340,13 @@ def run_ours(args) -> None:
         return np.linalg.norm(a - b, axis=1) / np.where(d > 0, d, 1.0)
 
     p99_vs_fp64 = float(np.percentile(rel(acc_mixed, acc64), 99))
-    direct = None
-    try:
-        import oracle
-        idx = np.random.default_rng(0xDEADBEEF).choice(args.n, 256, replace=False)
-        d = oracle.Oracle().direct(pos0, mass, targets=idx)
-        direct = {"p99_mixed": float(np.percentile(rel(acc_mixed[idx], d), 99)),
-                  "p99_fp64_bh": float(np.percentile(rel(acc64[idx], d), 99)),
-                  "sample": "256 particles, numpy default_rng(0xDEADBEEF)"}
-    except Exception as ex:  # the checker is optional here
-        direct = {"error": str(ex)}
+    idx = np.random.default_rng(0xDEADBEEF).choice(args.n, 4096, replace=False)
+    with nb.Engine(nb.default_params(device=local)) as ed:
+        ed.set_particles(pos0, np.zeros_like(pos0), mass)
+        d = ed.direct_forces(idx)  # the library's FP64 all-pairs kernel
+    direct = {"p99_mixed": float(np.percentile(rel(acc_mixed[idx], d), 99)),
+              "p99_fp64_bh": float(np.percentile(rel(acc64[idx], d), 99)),
+              "sample": "4096 particles, numpy default_rng(0xDEADBEEF); nbody_direct_forces (FP64, compensated)"}
 
     # ---- roofline of the fused walk kernel
     peak_tf, _ = nb.probe_fp32_peak(local)
@@ -367,6 +366,11 @@ def run_ours(args) -> None:
             cpu = {"value": v, "unit": UNIT, "cores": cpu_cores(), "kind": kind, "sample": desc}
         except Exception as ex:
             cpu = {"value": None, "unit": UNIT, "cores": cpu_cores(), "kind": "reference", "sample": f"failed: {ex}"}
+        if configs is not None:
+            try:
+                configs["cube5000"]["cpu_baseline"] = cube_reference(cube_inputs)
+            except Exception as ex:  # the reference harness is only on boxes where it was built
+                configs["cube5000"]["cpu_baseline"] = {"unavailable": str(ex)}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -469,8 +473,9 @@ def _timed_steps(eng, torch, stream, steps):
 
 def cube_leg(nb, torch, stream, device, frames=300):
     """Config 1: cube N=5000, size 512, masses U[5e10, 5e11], zero velocities,
-    seed 0xDEADBEEF, theta 0.5, dt 0.0333, 300 frames. Final positions against
-    the reference's own frame loop (oracle/_ref, serial build) where it is built."""
+    seed 0xDEADBEEF, theta 0.5, dt 0.0333, 300 frames. Returns the timings and the
+    final positions of both forms (compared with the reference's own frame loop
+    in the CPU-baseline leg)."""
     pos, vel, mass = nb.generate(5000, gen_type=0, size=512.0, seed=0xDEADBEEF)
     out = {"config": "cube N=5000 size=512 theta=0.5 dt=0.0333, 300 frames"}
     finals = {}
@@ -484,19 +489,25 @@ def cube_leg(nb, torch, stream, device, frames=300):
             e.step(frames)
             finals[name] = e.get_particles()[0]
         out[name] = {"ms_per_step": ms / frames, "steps_per_s": 1e3 * frames / ms}
-    try:
-        import oracle
-        import time
-        R = oracle.Reference()
-        t0 = time.perf_counter()
-        ref_pos, _, _ = R.run_frames(pos, vel, mass, frames, threads=1)
-        t1 = time.perf_counter()
-        scale = np.abs(ref_pos).max()
-        for name in finals:
-            out[name]["max_pos_err_vs_reference"] = float(np.abs(finals[name] - ref_pos).max() / scale)
-        out["reference_cpu"] = {"steps_per_s": frames / (t1 - t0), "cores": 1, "kind": "reference"}
-    except Exception as ex:  # the reference harness is optional on the box
-        out["reference_cpu"] = {"unavailable": str(ex)}
+    return out, (pos, vel, mass, finals)
+
+
+def cube_reference(inputs, frames=300):
+    """CPU-baseline leg of config 1: the reference's own frame loop (oracle/_ref,
+    serial build) on the same cube, timed on one host core; its final positions
+    are the check for the GPU runs."""
+    import time
+    import oracle
+    pos, vel, mass, finals = inputs
+    R = oracle.Reference()
+    t0 = time.perf_counter()
+    ref_pos, _, _ = R.run_frames(pos, vel, mass, frames, threads=1)
+    t1 = time.perf_counter()
+    scale = np.abs(ref_pos).max()
+    out = {"steps_per_s": frames / (t1 - t0), "cores": 1, "kind": "reference",
+           "sample": "cube N=5000, 300 frames, reference frame loop, 1 thread"}
+    for name, p in finals.items():
+        out[f"{name}_max_pos_err"] = float(np.abs(p - ref_pos).max() / scale)
     return out
 
 
@@ -527,17 +538,15 @@ def sphere_leg(nb, torch, stream, device, steps=100):
                      "energy_drift": (E1 - E0) / abs(E0),
                      "momentum_change": float(np.linalg.norm(np.subtract(d1["momentum"], d0["momentum"]))
                                               / max(P0, float(np.sum(mass)) * 1e-30))}
-    try:
-        import oracle
-        idx = np.random.default_rng(0xDEADBEEF).choice(len(mass), 4096, replace=False)
-        d = oracle.Oracle().direct(pos, mass, targets=idx)
-        nrm = np.linalg.norm(d, axis=1)
-        for name, a in accs.items():
-            out[name]["p99_err_vs_direct_sum"] = float(np.percentile(np.linalg.norm(a[idx] - d, axis=1) / nrm, 99))
-        out["mixed"]["p99_err_vs_fp64_form"] = float(np.percentile(
-            np.linalg.norm(accs["mixed"] - accs["fp64_form"], axis=1) / np.linalg.norm(accs["fp64_form"], axis=1), 99))
-    except Exception as ex:
-        out["direct_sum"] = {"unavailable": str(ex)}
+    idx = np.random.default_rng(0xDEADBEEF).choice(len(mass), 4096, replace=False)
+    with nb.Engine(nb.default_params(device=device)) as ed:
+        ed.set_particles(pos, vel, mass)
+        d = ed.direct_forces(idx)  # the library's FP64 all-pairs kernel
+    nrm = np.linalg.norm(d, axis=1)
+    for name, a in accs.items():
+        out[name]["p99_err_vs_direct_sum"] = float(np.percentile(np.linalg.norm(a[idx] - d, axis=1) / nrm, 99))
+    out["mixed"]["p99_err_vs_fp64_form"] = float(np.percentile(
+        np.linalg.norm(accs["mixed"] - accs["fp64_form"], axis=1) / np.linalg.norm(accs["fp64_form"], axis=1), 99))
     return out
 
 

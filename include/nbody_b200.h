@@ -220,6 +220,11 @@ typedef struct nbody_gen_params {
 void nbody_default_gen_params(nbody_gen_params *g);
 int nbody_generate(const nbody_gen_params *g, uint32_t n, double *pos, double *vel, double *mass);
 
+/* FP64 direct-sum (all-pairs) accelerations of the resident particles targets[0..m) (or of
+ * particles 0..m-1 when targets is NULL), with the reference's pair term (src/main.cpp:306-333)
+ * and compensated sums: the exact value that Barnes-Hut results are compared with. */
+int nbody_direct_forces(nbody_ctx *ctx, uint32_t m, const uint32_t *targets, int damping, double *acc_out);
+
 /* ---- frames and images -------------------------------------------------
  * The reference's frame files and renderer, on host arrays or the resident state. */
 

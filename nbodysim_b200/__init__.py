@@ -139,6 +139,7 @@ _SIGS = {
     "nbody_write_txt": (C.c_int, [C.c_char_p, C.c_uint32, C.c_void_p, C.c_int]),
     "nbody_find_resume_frame": (C.c_int, [C.c_char_p, C.c_uint32, C.POINTER(C.c_int32)]),
     "nbody_get_masses": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "nbody_direct_forces": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_int, C.c_void_p]),
     "nbody_save_frame": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint32, C.c_int, C.c_int, C.c_int]),
     "nbody_load_frame": (C.c_int, [C.c_void_p, C.c_char_p, C.c_uint32, C.c_int, C.POINTER(C.c_uint32)]),
     "nbody_default_image_params": (None, [C.POINTER(ImageParams)]),
@@ -321,6 +322,14 @@ class Engine:
         _check(self._lib.nbody_step(self._h, nsteps))
         if self.n and (self.params.collide or self.params.min_node_size > 0):
             self.n = self.device_view().n  # merging may have removed particles
+
+    def direct_forces(self, targets=None, damping: bool = False):
+        """FP64 all-pairs accelerations of the resident particles `targets` (default: all)."""
+        t = None if targets is None else np.ascontiguousarray(targets, dtype=np.uint32)
+        m = self.n if t is None else len(t)
+        out = np.zeros((m, 3))
+        _check(self._lib.nbody_direct_forces(self._h, m, _ptr(t), int(damping), out.ctypes.data))
+        return out
 
     def get_masses(self):
         m = np.zeros(self.n)

@@ -16,7 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libnbody_b200.so")
-SOURCES = ["api.cu", "tree.cu", "sort.cu", "walk.cu", "step.cu", "probe.cu", "noalloc.cu", "image.cu", "merge.cu", "generate.cpp", "io.cpp"]
+SOURCES = ["api.cu", "tree.cu", "sort.cu", "walk.cu", "step.cu", "probe.cu", "noalloc.cu", "image.cu", "merge.cu", "direct.cu", "generate.cpp", "io.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

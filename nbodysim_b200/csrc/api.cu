@@ -24,6 +24,7 @@
 #include "walk.cuh"
 #include "image.cuh"
 #include "merge.cuh"
+#include "direct.cuh"
 
 using namespace nbody;
 
@@ -121,6 +122,9 @@ struct nbody_ctx {
     uint2 *pairs = nullptr;
     uint32_t *hcounters = nullptr;  // pinned mirror of mb.counters
     uint64_t merged_min_size = 0, merged_collisions = 0, collision_pairs = 0;
+    // nbody_direct_forces: targets and results (grown on demand)
+    void *direct_arena = nullptr;
+    size_t direct_bytes = 0;
     // nbody_step_host: velocities uploaded on a second stream while the tree is built
     cudaStream_t aux_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_vel = nullptr;
@@ -920,6 +924,7 @@ int nbody_destroy(nbody_ctx *c) {
     if (c->sys_arena) cudaFree(c->sys_arena);
     if (c->img_arena) cudaFree(c->img_arena);
     if (c->merge_arena) cudaFree(c->merge_arena);
+    if (c->direct_arena) cudaFree(c->direct_arena);
     if (c->pairs) cudaFree(c->pairs);
     if (c->hcounters) cudaFreeHost(c->hcounters);
     if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
@@ -1398,6 +1403,38 @@ int nbody_load_frame(nbody_ctx *c, const char *dir, uint32_t num_frames, int dat
     int rc = nbody_set_particles(c, n, pos.data(), vel.data(), mass.data());
     if (rc) return rc;
     *next_frame = (uint32_t)f + 1;
+    return NBODY_OK;
+}
+
+int nbody_direct_forces(nbody_ctx *c, uint32_t m, const uint32_t *targets, int damping, double *acc_out) {
+    CTX_OR_FAIL(c);
+    if (!c->have_state) return fail(NBODY_ERR_STATE, "no particles set%s");
+    if (m && !acc_out) return fail(NBODY_ERR_INVALID, "acc_out is null%s");
+    if (!targets && m > c->n) return fail(NBODY_ERR_INVALID, "m exceeds the particle count%s");
+    if (targets)
+        for (uint32_t w = 0; w < m; w++)
+            if (targets[w] >= c->n) return fail(NBODY_ERR_INVALID, "target index out of range%s");
+    if (m == 0) return NBODY_OK;
+    const size_t need = align256(4 * (size_t)m) + align256(24 * (size_t)m);
+    if (need > c->direct_bytes) {
+        NB_CUDA(cudaStreamSynchronize(c->stream));
+        if (c->direct_arena) NB_CUDA(cudaFree(c->direct_arena));
+        c->direct_arena = nullptr;
+        c->direct_bytes = 0;
+        cudaError_t e = cudaMalloc(&c->direct_arena, need);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(NBODY_ERR_OOM, "direct-sum buffers (%s)", cudaGetErrorString(e));
+        }
+        c->direct_bytes = need;
+    }
+    uint32_t *d_t = (uint32_t *)c->direct_arena;
+    double *d_out = (double *)((char *)c->direct_arena + align256(4 * (size_t)m));
+    if (targets) NB_CUDA(cudaMemcpyAsync(d_t, targets, 4 * (size_t)m, cudaMemcpyHostToDevice, c->stream));
+    NB_CUDA(launch_direct(c->pos, c->mass, c->n, damping, targets ? d_t : nullptr, m, d_out, c->stream));
+    c->launches++;
+    NB_CUDA(cudaMemcpyAsync(acc_out, d_out, 24 * (size_t)m, cudaMemcpyDeviceToHost, c->stream));
+    NB_CUDA(cudaStreamSynchronize(c->stream));
     return NBODY_OK;
 }
 

@@ -158,3 +158,18 @@ def test_direct_sum_error_reported(nb, eng, orc):
     assert np.percentile(e, 99) < 5e-2
     ra, _ = orc.forces(pos, mass, 0.5)
     assert abs(np.percentile(rel(ra[idx], d), 99) - np.percentile(e, 99)) < 1e-5
+
+
+@pytest.mark.parametrize("damp", [False, True])
+def test_direct_sum_kernel_matches_oracle(nb, orc, damp):
+    """nbody_direct_forces (FP64, compensated) against the oracle's compensated direct sum."""
+    pos, vel, mass = nb.generate(6000, gen_type=1)
+    targets = np.random.default_rng(2).choice(6000, 300, replace=False).astype(np.uint32)
+    want = orc.direct(pos, mass, targets=targets, damping=damp)
+    with nb.Engine() as e:
+        e.set_particles(pos, vel, mass)
+        got = e.direct_forces(targets, damping=damp)
+        first = e.direct_forces(None)[:5]
+    scale = np.linalg.norm(want, axis=1)
+    assert (np.linalg.norm(got - want, axis=1) / scale).max() <= 1e-13
+    assert np.allclose(first, orc.direct(pos, mass, targets=np.arange(5, dtype=np.uint32)), rtol=1e-13, atol=0)
