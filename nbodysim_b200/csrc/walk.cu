@@ -532,6 +532,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
             // remaining nodes are decided lane by lane below.
             uint32_t my_open = 0;
             bool mixed = false;
+            float r2box = 0.f;  // squared distance of the node from the group's box (MIXED form)
             if (is_int) {
                 if constexpr (kFp64) {
                     const double sq = s.gc.S * so / theta;
@@ -557,6 +558,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                                 bz_ = fmaxf(fabsf(fcz - s.gc.box[4]), fabsf(fcz - s.gc.box[5]));
                     const float r2min = fmaf(az_, az_, fmaf(ay_, ay_, ax_ * ax_));
                     const float r2max = fmaf(bz_, bz_, fmaf(by_, by_, bx_ * bx_));
+                    r2box = r2min;
                     if (r2min <= 4.f * s.gc.tiny) mixed = true;
                     else if (r2min - qf > tol) my_open = 0;
                     else if (qf - r2max > tol) my_open = reach;
@@ -646,9 +648,13 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
             bool near = false;
             if constexpr (!kFp64) {
                 if (accm) {
-                    const float ax_ = fmaxf(fmaxf(s.gc.box[0] - fcx, fcx - s.gc.box[1]), 0.f), ay_ = fmaxf(fmaxf(s.gc.box[2] - fcy, fcy - s.gc.box[3]), 0.f),
-                                az_ = fmaxf(fmaxf(s.gc.box[4] - fcz, fcz - s.gc.box[5]), 0.f);
-                    near = fmaf(az_, az_, fmaf(ay_, ay_, ax_ * ax_)) < s.gc.near_r2;
+                    if (!is_int) {  // internal nodes have it from the group test
+                        const float ax_ = fmaxf(fmaxf(s.gc.box[0] - fcx, fcx - s.gc.box[1]), 0.f),
+                                    ay_ = fmaxf(fmaxf(s.gc.box[2] - fcy, fcy - s.gc.box[3]), 0.f),
+                                    az_ = fmaxf(fmaxf(s.gc.box[4] - fcz, fcz - s.gc.box[5]), 0.f);
+                        r2box = fmaf(az_, az_, fmaf(ay_, ay_, ax_ * ax_));
+                    }
+                    near = r2box < s.gc.near_r2;
                 }
             }
             const uint32_t am = __ballot_sync(FULL, accm != 0 && !near);
