@@ -533,6 +533,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
             uint32_t my_open = 0;
             bool mixed = false;
             float r2box = 0.f;  // squared distance of the node from the group's box (MIXED form)
+            float qf = 0.f, band = 0.f;  // (side/theta)^2 in FP32 and the half-width of its error band
             if (is_int) {
                 if constexpr (kFp64) {
                     const double sq = s.gc.S * so / theta;
@@ -550,8 +551,9 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                     else mixed = true;
                 } else {
                     const double sqd = s.gc.s_theta * so;
-                    const float qf = (float)(sqd * sqd), sqf = (float)sqd;
-                    const float tol = 2.f * fmaf(s.gc.pm_tol, sqf, kTolRel * qf);
+                    qf = (float)(sqd * sqd);
+                    band = fmaf(s.gc.pm_tol, (float)sqd, kTolRel * qf);
+                    const float tol = 2.f * band;
                     const float ax_ = fmaxf(fmaxf(s.gc.box[0] - fcx, fcx - s.gc.box[1]), 0.f), ay_ = fmaxf(fmaxf(s.gc.box[2] - fcy, fcy - s.gc.box[3]), 0.f),
                                 az_ = fmaxf(fmaxf(s.gc.box[4] - fcz, fcz - s.gc.box[5]), 0.f);
                     const float bx_ = fmaxf(fabsf(fcx - s.gc.box[0]), fabsf(fcx - s.gc.box[1])), by_ = fmaxf(fabsf(fcy - s.gc.box[2]), fabsf(fcy - s.gc.box[3])),
@@ -574,11 +576,8 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                     s.tc[lane] = make_double4(cx, cy, cz, s.gc.S * so);
                     s.tr[lane] = make_int2((int)reach, ref);
                 } else {
-                    const double sq = s.gc.s_theta * so;
-                    const float qf = (float)(sq * sq);
                     s.tc[lane] = make_float4(fcx, fcy, fcz, 0.f);
-                    s.tq[lane] = make_float4(qf, fmaf(s.gc.pm_tol, (float)sq, kTolRel * qf), __uint_as_float(reach),
-                                             __int_as_float(ref));
+                    s.tq[lane] = make_float4(qf, band, __uint_as_float(reach), __int_as_float(ref));
                 }
                 __syncwarp();
                 uint32_t mm = intm;
