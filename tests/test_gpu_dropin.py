@@ -17,6 +17,7 @@ pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB = os.path.join(ROOT, "oracle", "_ref", "libnbref_gpu.so")
+LIB_F32 = os.path.join(ROOT, "oracle", "_ref", "libnbref_gpu_f32.so")
 
 RUNNER = r'''
 import ctypes, sys
@@ -26,7 +27,7 @@ sys.exit(lib.ref_main(2, argv))
 '''
 
 
-def run_main(tmp, cuda, gen_type, precision=None, frames=4, n=3000):
+def run_main(tmp, cuda, gen_type, precision=None, frames=4, n=3000, lib=LIB, dtype=np.float64):
     d = tmp / ("gpu" if cuda else "cpu")
     (d / "data").mkdir(parents=True)
     cfg = d / "settings.cfg"
@@ -37,12 +38,12 @@ def run_main(tmp, cuda, gen_type, precision=None, frames=4, n=3000):
     env = dict(os.environ)
     if precision:
         env["NBODY_B200_PRECISION"] = precision
-    r = subprocess.run([sys.executable, "-c", RUNNER, LIB, str(cfg)], cwd=d, env=env, capture_output=True,
+    r = subprocess.run([sys.executable, "-c", RUNNER, lib, str(cfg)], cwd=d, env=env, capture_output=True,
                        text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     out = []
     for f in range(frames):
-        raw = np.fromfile(d / "data" / f"{f:04d}.dat", dtype=np.float64).reshape(-1, 10)
+        raw = np.fromfile(d / "data" / f"{f:04d}.dat", dtype=dtype).reshape(-1, 10).astype(np.float64)
         out.append(raw[np.argsort(raw[:, 9])])  # order by mass: unique per particle
     return out
 
@@ -67,3 +68,19 @@ def test_reference_main_with_gpu_shim_matches_cpu(dropin_lib, tmp_path, gen_type
         acc_c, acc_g = c[:, 6:9], g[:, 6:9]
         rel = np.linalg.norm(acc_c - acc_g, axis=1) / np.linalg.norm(acc_c, axis=1)
         assert np.percentile(rel, 99) <= (1e-12 if precision else 1e-5), (f, np.percentile(rel, 99))
+
+
+def test_float_build_main_with_gpu_shim(nb, tmp_path):
+    """The reference's FLOAT build with the shim: particles are widened to double
+    for the GPU (octants are then decided in double, not float), so the frames
+    agree with the FLOAT CPU path to float accuracy."""
+    if not os.path.exists(LIB_F32):
+        pytest.skip("oracle/_ref/libnbref_gpu_f32.so not built (needs the reference tree at build time)")
+    cpu = run_main(tmp_path / "f32", False, "cube", lib=LIB_F32, dtype=np.float32)
+    gpu = run_main(tmp_path / "f32", True, "cube", precision="fp64", lib=LIB_F32, dtype=np.float32)
+    for f, (c, g) in enumerate(zip(cpu, gpu)):
+        assert np.array_equal(c[:, 9], g[:, 9])
+        err = np.abs(c[:, 0:3] - g[:, 0:3]).max() / np.abs(c[:, 0:3]).max()
+        assert err <= 1e-5, (f, err)
+        rel = np.linalg.norm(c[:, 6:9] - g[:, 6:9], axis=1) / np.linalg.norm(c[:, 6:9], axis=1)
+        assert np.percentile(rel, 99) <= 1e-4, (f, np.percentile(rel, 99))
