@@ -118,3 +118,20 @@ def test_state_errors(nb):
         with pytest.raises(nb.NBodyError) as ex:
             e.step(1)
         assert ex.value.status == nb.ERR_STATE
+
+
+def test_step_host_on_a_caller_stream(nb):
+    """nbody_set_stream: the engine orders its work (and the overlapped velocity
+    upload of nbody_step_host) after the caller's stream."""
+    import ctypes
+    import torch
+    pos, vel, mass = nb.generate(70000, gen_type=2, size=1024.0)
+    s = torch.cuda.Stream()
+    with nb.Engine(adaptive=1) as e, nb.Engine(adaptive=1) as ref:
+        assert e._lib.nbody_set_stream(e._h, ctypes.c_void_p(s.cuda_stream)) == nb.OK
+        p1, v1 = pos.copy(), vel.copy()
+        e.step_host(p1, v1, mass, 2)
+        ref.set_particles(pos, vel, mass)
+        ref.step(2)
+        p2, v2 = ref.get_particles()
+    assert np.array_equal(p1, p2) and np.array_equal(v1, v2)
