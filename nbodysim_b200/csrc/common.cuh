@@ -72,6 +72,9 @@ struct Tree {
 __host__ __device__ inline int meta_level(int32_t m) { return m & 0xff; }
 __host__ __device__ inline int meta_nchild(int32_t m) { return (m >> 8) & 0xf; }
 
+// Exactly 2^-L for 0 <= L <= 1022 (cell sides halve exactly level by level).
+__device__ inline double exp2_neg(int L) { return __longlong_as_double((long long)(1023 - L) << 52); }
+
 // Non-negative doubles compare like their bit patterns.
 __device__ inline void atomic_max_nonneg(unsigned long long *a, double v) {
     atomicMax(a, (unsigned long long)__double_as_longlong(v));

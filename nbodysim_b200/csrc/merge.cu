@@ -36,9 +36,6 @@ namespace {
 constexpr uint32_t kUnionRetries = 1u << 20;
 constexpr int kFrames = kMaxLevels + 2;
 
-__device__ inline double exp2_neg(int L) {  // exactly 2^-L for 0 <= L <= 1022
-    return __longlong_as_double((long long)(1023 - L) << 52);
-}
 
 struct Val {
     double x, y, z, vx, vy, vz, m;

@@ -45,9 +45,6 @@ __device__ inline float rsqrt_ftz(float x) {
     return y;
 }
 
-__device__ inline double exp2_neg(int L) {  // exactly 2^-L for 0 <= L <= 1022
-    return __longlong_as_double((long long)(1023 - L) << 52);
-}
 
 // Per-warp shared memory. The stack holds nodes still to be examined with
 // the mask of lanes that reached them; the tile holds the up-to-32 internal
