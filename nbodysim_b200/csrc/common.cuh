@@ -71,6 +71,7 @@ struct Tree {
 
 __host__ __device__ inline int meta_level(int32_t m) { return m & 0xff; }
 __host__ __device__ inline int meta_nchild(int32_t m) { return (m >> 8) & 0xf; }
+__host__ __device__ inline int meta_ninternal(int32_t m) { return (m >> 12) & 0xf; }  // children that are nodes
 
 // Exactly 2^-L for 0 <= L <= 1022 (cell sides halve exactly level by level).
 __device__ inline double exp2_neg(int L) { return __longlong_as_double((long long)(1023 - L) << 52); }

@@ -439,7 +439,7 @@ __global__ void k_collapse(const int32_t *__restrict__ bleft, const int32_t *__r
     // In-order walk over the same-level binary nodes (at most 7 of them):
     // a frame visits its left child, then its right child.
     int fnode[8], fstate[8];
-    int fs = 0, nch = 0;
+    int fs = 0, nch = 0, nint = 0;
     fnode[0] = (int)i; fstate[0] = 0; fs = 1;
     while (fs > 0) {
         const int x = fnode[fs - 1];
@@ -457,20 +457,22 @@ __global__ void k_collapse(const int32_t *__restrict__ bleft, const int32_t *__r
                 const int cid = (int)head_id[ch];
                 ochild[8 * id + nch] = cid;
                 oparent[cid] = id;
+                nint++;
             }
             nch++;
         } else {
             atomicOr(&sc->status, kStatusCapacity);
         }
     }
-    ometa[id] = L | (min(nch, 8) << 8);
+    ometa[id] = L | (min(nch, 8) << 8) | (min(nint, 8) << 12);
     if (id == 0) oparent[0] = -1;
     atomicMax(&sc->depth, (uint32_t)L);
 }
 
 // ---------------------------------------------------------------------------
-// Bottom-up mass and centre of mass (src/octree.cpp:203-221, 252-278): one
-// thread per leaf climbs while it is the last child to finish. Sums run in
+// Bottom-up mass and centre of mass (src/octree.cpp:203-221, 252-278): the
+// climb starts at the nodes whose children are all bodies, and a node is
+// computed by the thread of its last node child to finish. Sums run in
 // child order with explicit round-to-nearest operations (no FMA contraction),
 // as the reference computes them. A child separated from its parent by k
 // single-child chain nodes enters with its centre of mass passed k times
@@ -486,9 +488,12 @@ __global__ void k_com(const double4 *__restrict__ body, const int32_t *__restric
                       const int32_t *__restrict__ oparent, const int32_t *__restrict__ ochild,
                       const int32_t *__restrict__ ometa, double4 *onode, uint32_t *ocount,
                       uint32_t n, DevScalars *sc) {
-    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    int p = leaf_oparent[j];
+    // One thread per node; the climb starts at nodes whose children are all
+    // bodies, and a node is computed by the last of its node children to finish.
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n - 1 || q >= sc->n_onodes) return;
+    int p = (int)q;
+    if (meta_ninternal(ometa[p]) != 0) return;
     // A well-formed tree is at most kMaxLevels + 1 internal levels deep; the
     // bound only guards against a malformed tree after a reported error.
     for (int hops = 0; p >= 0; hops++) {
@@ -498,12 +503,14 @@ __global__ void k_com(const double4 *__restrict__ body, const int32_t *__restric
         }
         const int32_t meta = ometa[p];
         const int nch = meta_nchild(meta);
-        // One acquire-release count: it publishes the node this thread wrote on
-        // the previous hop, and the last child to arrive sees every other
-        // child's result.
-        uint32_t old;
-        asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(&ocount[p]) : "memory");
-        if (old != (uint32_t)(nch - 1)) return;
+        if (hops > 0) {
+            // One acquire-release count: it publishes the node this thread wrote on
+            // the previous hop, and the last node child to arrive sees every
+            // other child's result.
+            uint32_t old;
+            asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(&ocount[p]) : "memory");
+            if (old != (uint32_t)(meta_ninternal(meta) - 1)) return;
+        }
         // The reference sums the masses, then the mass-weighted centres, each in
         // child order; both sums run here in one pass over the children.
         const int L = meta_level(meta);
@@ -630,7 +637,7 @@ cudaError_t compute_com(const TreeBuild &tb, cudaStream_t st, unsigned *launches
     if (n < 2) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(tb.ocount, 0, sizeof(uint32_t) * (n - 1), st);
     if (e != cudaSuccess) return e;
-    k_com<<<blocks_for(n, 256), 256, 0, st>>>(tb.body, tb.leaf_oparent, tb.oparent, tb.ochild, tb.ometa,
+    k_com<<<blocks_for(n - 1, 256), 256, 0, st>>>(tb.body, tb.leaf_oparent, tb.oparent, tb.ochild, tb.ometa,
                                               tb.onode, tb.ocount, n, tb.sc);
     *launches += 1;
     return cudaGetLastError();
