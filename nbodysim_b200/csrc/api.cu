@@ -125,9 +125,10 @@ struct nbody_ctx {
     // nbody_direct_forces: targets and results (grown on demand)
     void *direct_arena = nullptr;
     size_t direct_bytes = 0;
-    // nbody_step_host: velocities uploaded on a second stream while the tree is built
+    // nbody_step_host: masses and velocities uploaded on a second stream while the tree is built
     cudaStream_t aux_stream = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_vel = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_mass = nullptr, ev_vel = nullptr;
+    cudaEvent_t mass_pending = nullptr;  // set while a force pass must wait for ev_mass before reading masses
 };
 
 namespace {
@@ -253,6 +254,7 @@ void tree_inputs(nbody_ctx *c, uint32_t n, bool want_vmax) {
     tb.n = n;
     tb.pos = c->pos;
     tb.mass = c->mass;
+    tb.mass_ready = c->mass_pending;
     tb.vel_for_max = want_vmax ? c->vel : nullptr;
     tb.sc = c->sc;
 }
@@ -929,6 +931,7 @@ int nbody_destroy(nbody_ctx *c) {
     if (c->hcounters) cudaFreeHost(c->hcounters);
     if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_mass) cudaEventDestroy(c->ev_mass);
     if (c->ev_vel) cudaEventDestroy(c->ev_vel);
     if (c->sc) cudaFree(c->sc);
     if (c->hsc) cudaFreeHost(c->hsc);
@@ -1138,30 +1141,42 @@ int nbody_step_host(nbody_ctx *c, uint32_t n, double *pos, double *vel, const do
     if (n == 0) return NBODY_OK;
     int rc;
     if (n >= kOverlapMin && nsteps > 0) {
-        // Positions and masses first (the tree needs them); the velocities cross
-        // on a second stream while the first force pass runs, and are waited for
-        // just before that step's update.
+        // Positions first: the root cube, keys and sort need nothing else. The
+        // masses (first read when the sorted bodies are gathered) and then the
+        // velocities (first read by the update) cross on a second stream while
+        // the first force pass runs.
         if ((rc = reserve(c, n))) return rc;
         if (!c->aux_stream) {
             NB_CUDA(cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking));
             NB_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+            NB_CUDA(cudaEventCreateWithFlags(&c->ev_mass, cudaEventDisableTiming));
             NB_CUDA(cudaEventCreateWithFlags(&c->ev_vel, cudaEventDisableTiming));
         }
-        // The velocity copy starts once the positions and masses are in, so that it
-        // does not share the host link with them.
+        // The second stream's copies start once the positions are in, so that they
+        // do not share the host link with them.
         NB_CUDA(cudaMemcpyAsync(c->pos, pos, 24 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
-        NB_CUDA(cudaMemcpyAsync(c->mass, mass, 8 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
         NB_CUDA(cudaEventRecord(c->ev_fork, c->stream));
         NB_CUDA(cudaStreamWaitEvent(c->aux_stream, c->ev_fork, 0));
+        NB_CUDA(cudaMemcpyAsync(c->mass, mass, 8 * (size_t)n, cudaMemcpyHostToDevice, c->aux_stream));
+        NB_CUDA(cudaEventRecord(c->ev_mass, c->aux_stream));
         NB_CUDA(cudaMemcpyAsync(c->vel, vel, 24 * (size_t)n, cudaMemcpyHostToDevice, c->aux_stream));
         NB_CUDA(cudaEventRecord(c->ev_vel, c->aux_stream));
         c->n = n;
         c->have_state = c->have_vel = true;
         c->have_acc = false;
-        if ((rc = begin_call(c))) return rc;
+        if ((rc = begin_call(c))) {
+            NB_CUDA(cudaStreamWaitEvent(c->stream, c->ev_vel, 0));
+            return rc;
+        }
         const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
         StepParams sp{c->p.dt, c->p.adaptive, c->p.min_adaptive_dt, c->p.max_pos_change, c->p.max_vel_change};
-        if ((rc = force_pass(c, c->p.damping, c->p.theta, fp64, false, false, false, false))) return rc;
+        c->mass_pending = c->ev_mass;
+        rc = force_pass(c, c->p.damping, c->p.theta, fp64, false, false, false, false);
+        c->mass_pending = nullptr;
+        if (rc) {
+            NB_CUDA(cudaStreamWaitEvent(c->stream, c->ev_vel, 0));
+            return rc;
+        }
         NB_CUDA(cudaStreamWaitEvent(c->stream, c->ev_vel, 0));
         if (c->p.adaptive) {
             NB_CUDA(launch_maxima(c->acc, fp64, c->vel, n, c->sc, c->stream));

@@ -17,11 +17,10 @@ namespace nbody {
 // ---------------------------------------------------------------------------
 // Root cube: bbox midpoint; side = largest extent + 2.0, a tie for the largest
 // extent falls through to the z extent (src/main.cpp:898-920). Also flags
-// non-finite positions or masses, and (optionally) reduces max |v| for the
-// adaptive step.
-__global__ void k_bbox(const double *__restrict__ pos, const double *__restrict__ vel,
-                       const double *__restrict__ mass, uint32_t n, double *__restrict__ partial,
-                       DevScalars *sc, int keep_root) {
+// non-finite positions (masses are checked where the bodies are gathered), and
+// (optionally) reduces max |v| for the adaptive step.
+__global__ void k_bbox(const double *__restrict__ pos, const double *__restrict__ vel, uint32_t n,
+                       double *__restrict__ partial, DevScalars *sc, int keep_root) {
     __shared__ double s_red[7][32];
     __shared__ bool s_last;
     double mn[3] = {INFINITY, INFINITY, INFINITY};
@@ -30,8 +29,7 @@ __global__ void k_bbox(const double *__restrict__ pos, const double *__restrict_
     bool bad = false;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double x = pos[3 * (size_t)i], y = pos[3 * (size_t)i + 1], z = pos[3 * (size_t)i + 2];
-        double m = mass[i];
-        bad |= !(isfinite(x) && isfinite(y) && isfinite(z) && isfinite(m));
+        bad |= !(isfinite(x) && isfinite(y) && isfinite(z));
         mn[0] = fmin(mn[0], x); mx[0] = fmax(mx[0], x);
         mn[1] = fmin(mn[1], y); mx[1] = fmax(mx[1], y);
         mn[2] = fmin(mn[2], z); mx[2] = fmax(mx[2], z);
@@ -269,13 +267,16 @@ unsigned scan_exclusive(uint32_t *v, uint32_t len, uint32_t *tile_sums, uint32_t
 }
 
 // ---------------------------------------------------------------------------
+// Bodies in sorted order; flags non-finite masses.
 __global__ void k_gather_bodies(const uint32_t *__restrict__ idx, const double *__restrict__ pos,
                                 const double *__restrict__ mass, double4 *__restrict__ body,
-                                uint32_t n) {
+                                uint32_t n, DevScalars *sc) {
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     uint32_t i = idx[j];
-    body[j] = make_double4(pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2], mass[i]);
+    const double m = mass[i];
+    if (!isfinite(m)) atomicOr(&sc->status, kStatusNonFinite);
+    body[j] = make_double4(pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2], m);
 }
 
 // Groups of particles whose 42-level keys agree get a third key word (levels
@@ -566,9 +567,10 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
     if (n == 0) return cudaSuccess;
     const bool multi = tb.nsys > 1;
     // root cube (+ max |v| when requested); one per system when there are several
-    k_bbox<<<tb.bbox_blocks, 256, 0, st>>>(tb.pos, tb.vel_for_max, tb.mass, n, tb.bbox_partial, tb.sc,
+    k_bbox<<<tb.bbox_blocks, 256, 0, st>>>(tb.pos, tb.vel_for_max, n, tb.bbox_partial, tb.sc,
                                            multi ? 0 : tb.keep_root);
     if (multi) {
+        if (tb.mass_ready) cudaStreamWaitEvent(st, tb.mass_ready, 0);
         k_bbox_systems<<<tb.nsys, 256, 0, st>>>(tb.pos, tb.mass, tb.sys_start, tb.sys_root, tb.sc);
         L += 1;
     }
@@ -600,7 +602,8 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
         L += 3;
     }
     k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key2, tb.idx_a, tb.key_a, n);  // k2 sorted
-    k_gather_bodies<<<blocks_for(n, 256), 256, 0, st>>>(tb.idx_a, tb.pos, tb.mass, tb.body, n);
+    if (tb.mass_ready && !multi) cudaStreamWaitEvent(st, tb.mass_ready, 0);  // the first reader of the masses
+    k_gather_bodies<<<blocks_for(n, 256), 256, 0, st>>>(tb.idx_a, tb.pos, tb.mass, tb.body, n, tb.sc);
     L += 3;
     *launches += L;
     if (n < 2) return cudaGetLastError();

@@ -9,6 +9,8 @@ struct TreeBuild {
     uint32_t n;
     const double *pos;          // user order, AoS
     const double *mass;
+    cudaEvent_t mass_ready;     // non-null: the masses are still being copied on another stream;
+                                // the build waits for this event before it first reads them
     const double *vel_for_max;  // non-null: also reduce max |v| (adaptive dt)
     int keep_root;              // rebuild inside the root cube already in sc (single system)
     DevScalars *sc;

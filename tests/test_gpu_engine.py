@@ -30,8 +30,8 @@ def test_frames_match_oracle_mixed(nb, orc):
 
 @pytest.mark.parametrize("adaptive", [0, 1])
 def test_step_host_overlapped_upload_equals_resident(nb, adaptive):
-    """From 65,536 particles nbody_step_host uploads the velocities on a second
-    stream during the force pass; the result must not change."""
+    """From 65,536 particles nbody_step_host uploads the masses and velocities on
+    a second stream during the force pass; the result must not change."""
     pos, vel, mass = nb.generate(70000, gen_type=1, min_vel=0.0, max_vel=2.0)
     with nb.Engine(adaptive=adaptive) as e:
         e.set_particles(pos, vel, mass)
@@ -43,6 +43,22 @@ def test_step_host_overlapped_upload_equals_resident(nb, adaptive):
         e.step_host(p2, v2, mass, 1)
         dt2 = e.stats()["last_dt"]
     assert np.array_equal(p1, p2) and np.array_equal(v1, v2) and dt1 == dt2
+
+
+def test_step_host_overlapped_nonfinite_mass(nb):
+    """A non-finite mass that arrives on the second stream is still reported, and
+    the context stays usable."""
+    pos, vel, mass = nb.generate(70000, gen_type=1)
+    bad = mass.copy()
+    bad[12345] = np.nan
+    with nb.Engine() as e:
+        p, v = pos.copy(), vel.copy()
+        with pytest.raises(nb.NBodyError) as ex:
+            e.step_host(p, v, bad, 1)
+        assert ex.value.status == nb.ERR_NONFINITE
+        p, v = pos.copy(), vel.copy()
+        e.step_host(p, v, mass, 1)
+        assert np.isfinite(p).all() and np.isfinite(v).all()
 
 
 def test_step_host_equals_resident(nb):

@@ -144,8 +144,9 @@ def test_nonfinite_rejected(nb, eng):
     assert e.value.status == nb.ERR_NONFINITE
     mass[3] = np.inf
     pos[10, 1] = 0.0
-    with pytest.raises(nb.NBodyError):
+    with pytest.raises(nb.NBodyError) as e:
         eng.barnes_hut(pos, mass)
+    assert e.value.status == nb.ERR_NONFINITE
 
 
 def test_direct_sum_error_reported(nb, eng, orc):
