@@ -10,7 +10,8 @@ cube -> Morton keys -> radix sort -> octree -> mass/COM -> fused walk + gravity
   value        interactions/s over K resident steps (inputs already in HBM),
                CUDA events on the engine's stream, max over ranks
   e2e          the same metric through the C ABI with host buffers: every step
-               uploads pos/vel/mass from pinned memory and downloads pos/vel
+               uploads pos/vel/mass from pinned memory and downloads pos/vel;
+               the same K steps from the same state as `value`
   roofline     the fused walk kernel: 20 FLOP per interaction (the customary
                N-body count) against the measured FP32 FMA peak
   cpu_baseline the reference's own CPU walk (oracle/_ref, all host threads) on a
@@ -229,6 +230,7 @@ def run_ours(args) -> None:
     # ---- resident steps (device-timed)
     eng.set_particles(pos0, vel0, mass)
     eng.step(args.warmup)
+    pos_w, vel_w = eng.get_particles()  # the e2e leg times the same K steps from this state
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
@@ -266,10 +268,10 @@ def run_ours(args) -> None:
     hp = torch.empty((args.n, 3), dtype=torch.float64, pin_memory=True).numpy()
     hv = torch.empty((args.n, 3), dtype=torch.float64, pin_memory=True).numpy()
     hm = torch.empty((args.n,), dtype=torch.float64, pin_memory=True).numpy()
-    hp[:] = pos0; hv[:] = vel0; hm[:] = mass
+    hp[:] = pos_w; hv[:] = vel_w; hm[:] = mass
     for _ in range(max(1, args.warmup // 2)):
         eng.step_host(hp, hv, hm, 1)
-    hp[:] = pos0; hv[:] = vel0
+    hp[:] = pos_w; hv[:] = vel_w
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
