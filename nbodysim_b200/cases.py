@@ -1,7 +1,7 @@
 """Fixed workloads for profiling one kernel under ncu (device code is this package's).
 
-    python -m nbodysim_b200.cases walk --gen shell --n 1048576 --evolve 30 --save gpurun_out/shell30.npz
-    python -m nbodysim_b200.cases walk --load gpurun_out/shell30.npz --passes 2
+    python -m nbodysim_b200.cases walk --gen shell --n 1048576 --evolve 30 --save /tmp/shell30.npz
+    python -m nbodysim_b200.cases walk --load /tmp/shell30.npz --passes 2
 
 The first form generates the seeded reference initial conditions, advances them
 `--evolve` steps with adaptive dt (the bench's regime), optionally saves the
