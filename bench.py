@@ -14,8 +14,9 @@ cube -> Morton keys -> radix sort -> octree -> mass/COM -> fused walk + gravity
                the same K steps from the same state as `value`
   roofline     the fused walk kernel: 20 FLOP per interaction (the customary
                N-body count) against the measured FP32 FMA peak
-  cpu_baseline the reference's own CPU walk (oracle/_ref, all host threads) on a
-               bounded sample of the same workload; also the reference's frame
+  cpu_baseline the reference's own CPU walk (oracle/_ref, all host threads, and
+               one thread under `single_thread`) on a bounded sample of the
+               same workload; also the reference's frame
                loop on config 1, which checks the GPU's final positions
 
 `--impl reference` times the reference's CPU implementation alone (rank 0).
@@ -366,6 +367,9 @@ def run_ours(args) -> None:
         try:
             v, desc, kind, _ = cpu_reference_sample(pos0, mass, args.theta, args.cpu_seconds, cpu_cores(), counts)
             cpu = {"value": v, "unit": UNIT, "cores": cpu_cores(), "kind": kind, "sample": desc}
+            # the same measurement on one thread, for the per-core rate
+            v1, desc1, _, _ = cpu_reference_sample(pos0, mass, args.theta, min(args.cpu_seconds, 8.0), 1, counts)
+            cpu["single_thread"] = {"value": v1, "unit": UNIT, "cores": 1, "sample": desc1}
         except Exception as ex:
             cpu = {"value": None, "unit": UNIT, "cores": cpu_cores(), "kind": "reference", "sample": f"failed: {ex}"}
         if configs is not None:
