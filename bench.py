@@ -367,11 +367,15 @@ def run_ours(args) -> None:
         try:
             v, desc, kind, _ = cpu_reference_sample(pos0, mass, args.theta, args.cpu_seconds, cpu_cores(), counts)
             cpu = {"value": v, "unit": UNIT, "cores": cpu_cores(), "kind": kind, "sample": desc}
-            # the same measurement on one thread, for the per-core rate
-            v1, desc1, _, _ = cpu_reference_sample(pos0, mass, args.theta, min(args.cpu_seconds, 8.0), 1, counts)
-            cpu["single_thread"] = {"value": v1, "unit": UNIT, "cores": 1, "sample": desc1}
         except Exception as ex:
             cpu = {"value": None, "unit": UNIT, "cores": cpu_cores(), "kind": "reference", "sample": f"failed: {ex}"}
+        if cpu["value"] is not None:
+            # the same measurement on one thread, for the per-core rate
+            try:
+                v1, desc1, _, _ = cpu_reference_sample(pos0, mass, args.theta, min(args.cpu_seconds, 8.0), 1, counts)
+                cpu["single_thread"] = {"value": v1, "unit": UNIT, "cores": 1, "sample": desc1}
+            except Exception as ex:
+                cpu["single_thread"] = {"value": None, "sample": f"failed: {ex}"}
         if configs is not None:
             try:
                 configs["cube5000"]["cpu_baseline"] = cube_reference(cube_inputs)
