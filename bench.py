@@ -354,6 +354,11 @@ def run_ours(args) -> None:
     # ---- roofline of the fused walk kernel
     peak_tf, _ = nb.probe_fp32_peak(local)
     achieved = FLOP_PER_INTERACTION * walk_inter / (walk_ms * 1e-3) / 1e12
+    # nominal FP32 peak for comparison: SMs x 128 lanes x 2 FLOP x the maximum SM clock
+    clocks = clk.summary()
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    max_mhz = clocks.get("sm_max_mhz") if isinstance(clocks, dict) else None
+    peak_nominal = sms * 128 * 2 * max_mhz * 1e6 / 1e12 if max_mhz else None
     traffic = None
     prof = os.path.join(ROOT, "profiles", "walk_traffic.json")
     if os.path.exists(prof):
@@ -400,7 +405,7 @@ def run_ours(args) -> None:
         "adjoint": adjoint,
         "ensemble": ensemble,
         "configs": configs,
-        "clocks": clk.summary(),
+        "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 56 * args.n,
                 "d2h_bytes_per_step": 48 * args.n},
         "gpu_launches": int(launches),
@@ -409,7 +414,9 @@ def run_ours(args) -> None:
                      "frac": achieved / peak_tf if peak_tf else None, "traffic": traffic,
                      "kernel": "k_walk (fused walk + gravity)",
                      "peak_source": "measured FP32 FMA probe (nbody_probe_fp32_peak); MEASURED_PEAKS.json has no FP32 figure",
-                     "flop_per_interaction": FLOP_PER_INTERACTION},
+                     "flop_per_interaction": FLOP_PER_INTERACTION,
+                     "peak_nominal": peak_nominal,
+                     "peak_nominal_basis": f"{sms} SMs x 128 FP32 lanes x 2 FLOP x {max_mhz} MHz (clocks.max.sm)"},
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
