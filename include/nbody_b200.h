@@ -121,7 +121,9 @@ int nbody_step(nbody_ctx *ctx, uint32_t nsteps);
 /* Forces only, on the resident state (acc stays on the device). */
 int nbody_compute_forces(nbody_ctx *ctx);
 /* One step with host buffers in and out: upload pos/vel/mass, step, download pos/vel.
- * pos/vel are updated in place. */
+ * pos/vel are updated in place. From 65,536 particles the masses and velocities
+ * are copied on a second stream while the first step's tree is built; with pinned
+ * host buffers that copy overlaps the GPU work. */
 int nbody_step_host(nbody_ctx *ctx, uint32_t n, double *pos, double *vel, const double *mass,
                     uint32_t nsteps);
 
