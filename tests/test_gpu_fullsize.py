@@ -8,7 +8,9 @@ magnitude and the second key word decides most of the tree.
   (MIXED) and 1e-12 max (FP64 form).
 - Over all N particles: the MIXED and FP64 forms accept the same nodes for every
   particle (both make the reference's decisions), the counts add up to the
-  interaction statistic, and MIXED stays within p99 1e-5 of the FP64 form."""
+  interaction statistic, and MIXED stays within p99 1e-5 of the FP64 form.
+- With damping on the sample; and the sphere of 100,000 particles, every
+  particle against the oracle."""
 import numpy as np
 import pytest
 
@@ -77,3 +79,20 @@ def test_forms_agree_on_every_particle(states, eng, eng64, state):
     assert inter == int(cnt.sum(dtype=np.uint64)) == eng64.stats()["interactions"]
     assert np.isfinite(acc).all()
     assert np.percentile(rel(acc, a64), 99) <= P99_MIXED
+
+
+def test_damped_sample_against_oracle(states, sample, eng, orc):
+    pos, mass = states["initial"]
+    acc, cnt = eng.barnes_hut(pos, mass, damping=True, theta=0.5, counts=True)
+    ra, rc = orc.forces(pos, mass, 0.5, damping=True, sample=sample)
+    assert np.array_equal(cnt[sample], rc)
+    assert np.percentile(rel(acc[sample], ra), 99) <= P99_MIXED
+
+
+def test_sphere_100k_every_particle(nb, eng, orc):
+    """The sphere of 100,000 particles (r 100, rotation 0.1): every particle against the oracle."""
+    pos, _, mass = nb.generate(100_000, gen_type=nb.SPHERE, size=1024.0, r_sphere=100.0, rotation_magnitude=0.1)
+    acc, cnt = eng.barnes_hut(pos, mass, theta=0.5, counts=True)
+    ra, rc = orc.forces(pos, mass, 0.5)
+    assert np.array_equal(cnt, rc), f"{np.count_nonzero(cnt != rc)} particles differ"
+    assert np.percentile(rel(acc, ra), 99) <= P99_MIXED
