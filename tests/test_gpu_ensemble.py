@@ -113,3 +113,30 @@ def test_autotune_picks_a_valid_shape_and_keeps_results(nb):
         e.set_particles(pos, vel, mass)
         e.step(2)
         assert e.stats()["walk_warps_per_block"] in (1, 2, 4)
+
+
+def test_ensemble_at_full_scale(nb, orc):
+    """512 systems, N per system log-uniform in [1024, 65536] (~9M particles), gen
+    type cycling cube/sphere/shell: one force pass over the ensemble. Six systems
+    (the smallest, the largest and four seeded picks) must equal their own runs bit
+    for bit, and two of them the oracle's accepted-node counts."""
+    rng = np.random.default_rng(0xDEADBEEF)
+    counts = np.exp(rng.uniform(np.log(1024), np.log(65536), 512)).astype(np.uint32)
+    parts = [nb.generate(int(c), gen_type=s % 3, size=512.0 if s % 3 == 0 else 1024.0, seed=0xDEADBEEF + s)
+             for s, c in enumerate(counts)]
+    pos = np.concatenate([p[0] for p in parts]); vel = np.concatenate([p[1] for p in parts])
+    mass = np.concatenate([p[2] for p in parts])
+    offs = np.concatenate([[0], np.cumsum(counts.astype(np.int64))])
+    picks = sorted({int(np.argmin(counts)), int(np.argmax(counts)), *map(int, rng.choice(512, 4, replace=False))})
+    with nb.Engine() as e:
+        e.set_systems(counts)
+        e.set_particles(pos, vel, mass)
+        e.compute_forces()
+        _, _, acc = e.get_particles(acc=True)
+        for k, s in enumerate(picks):
+            p, _, m = parts[s]
+            a, cnt = e.barnes_hut(p, m, counts=True)
+            assert np.array_equal(acc[offs[s]:offs[s + 1]], a), s
+            if k < 2:
+                _, rc = orc.forces(p, m, 0.5)
+                assert np.array_equal(cnt, rc), s
