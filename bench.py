@@ -457,7 +457,9 @@ def adjoint_leg(nb, torch, stream, device, fd_coords=0):
         fwd_ck = ev[2].elapsed_time(ev[3])
         bwd = ev[4].elapsed_time(ev[5])
         out.update(forward_ms=fwd, forward_checkpointed_ms=fwd_ck, backward_ms=bwd, ratio=bwd / fwd,
-                   loss=float(((xK - target) ** 2).sum() / n))
+                   loss=float(((xK - target) ** 2).sum() / n),
+                   gradients_finite=bool(np.isfinite(gp).all() and np.isfinite(gv).all() and np.isfinite(gm).all()),
+                   max_abs_dL_dpos0=float(np.abs(gp).max()))
         if fd_coords:
             rng = np.random.default_rng(0xDEADBEEF)
             idx = rng.choice(3 * n, fd_coords, replace=False)

@@ -751,7 +751,8 @@ int adjoint_force(nbody_ctx *c, const double *pos, int damping, double theta, bo
     int rc = force_pass(c, damping, theta, fp64, false, false, false, false, pos, true, nullptr, false, -1, restore_slot);
     if (rc) return rc;
     NB_CUDA(launch_adj_distribute(c->tb.body, c->tb.idx_a, c->tb.leaf_oparent, c->tb.oparent, c->tb.onode,
-                                  c->adj_node, c->adj_leaf, c->gdir, fp64, c->lx, c->lm, c->n, c->stream));
+                                  c->adj_node, c->adj_leaf, c->gdir, fp64, fp64 ? nullptr : &c->sc->lam_scale, c->lx,
+                                  c->lm, c->n, c->stream));
     c->launches++;
     return NBODY_OK;
 }
@@ -1260,8 +1261,8 @@ int nbody_force_vjp(nbody_ctx *c, uint32_t n, const double *pos, const double *m
     if (fp64) {
         NB_CUDA(cudaMemcpyAsync(c->lam, c->lx, 24 * (size_t)n, cudaMemcpyDeviceToDevice, c->stream));
     } else {
-        NB_CUDA(launch_double_to_float(c->lx, (float *)c->lam, 3 * (size_t)n, c->stream));
-        c->launches++;
+        NB_CUDA(launch_lam_to_float_scaled(c->lx, (float *)c->lam, 3 * (size_t)n, c->sc, c->stream));
+        c->launches += 2;
     }
     NB_CUDA(cudaMemsetAsync(c->lx, 0, 24 * (size_t)n, c->stream));
     NB_CUDA(cudaMemsetAsync(c->lm, 0, 8 * (size_t)n, c->stream));
@@ -1358,8 +1359,16 @@ int nbody_backward(nbody_ctx *c, const double *dL_dpos, const double *dL_dvel, d
         }
         for (int i = (int)len - 1; i >= 0; i--) {
             auto adj = [&, i]() -> int {
-                NB_CUDA(launch_adj_pre(c->lx, c->lv, c->lam, fp64, c->p.dt, n, c->stream));
-                c->launches++;
+                if (fp64) {
+                    NB_CUDA(launch_adj_pre(c->lx, c->lv, c->lam, true, c->p.dt, n, c->stream));
+                    c->launches++;
+                } else {
+                    // dL/da in FP64 (gdir is free until the walk), then scaled into FP32
+                    double *lam_d = c->gdir;
+                    NB_CUDA(launch_adj_pre(c->lx, c->lv, lam_d, true, c->p.dt, n, c->stream));
+                    NB_CUDA(launch_lam_to_float_scaled(lam_d, (float *)c->lam, N3, c->sc, c->stream));
+                    c->launches += 3;
+                }
                 // positions 0 .. len-2 of the segment had their octrees saved by the recomputation
                 const int restore = (uint32_t)i + 1 < len && (uint32_t)i < c->n_slots ? i : -1;
                 return adjoint_force(c, c->seg_pos + N3 * (size_t)i, c->p.damping, c->p.theta, fp64, restore);

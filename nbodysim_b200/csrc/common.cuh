@@ -56,6 +56,11 @@ struct DevScalars {
     unsigned long long max_acc_bits;  // max |a| (non-negative double as ordered bits)
     unsigned long long max_vel_bits;  // max |v|
     double dt_used;
+    // MIXED adjoint: the FP32 cotangents are the FP64 ones times 2^-e, with 2^e
+    // the power of two that brings the largest into [0.5, 1); results are
+    // multiplied back by lam_scale = 2^e in FP64.
+    unsigned long long lam_max_bits;  // max |cotangent| (non-negative double as ordered bits)
+    double lam_scale;
     double diag[16];          // kinetic, potential, momentum[3], L[3], mass, m*x[3]
 };
 

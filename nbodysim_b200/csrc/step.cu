@@ -136,7 +136,8 @@ __global__ void k_adj_distribute(const double4 *__restrict__ body, const uint32_
                                  const int32_t *__restrict__ leaf_oparent, const int32_t *__restrict__ oparent,
                                  const double4 *__restrict__ onode, const double *__restrict__ adj_node,
                                  const double *__restrict__ adj_leaf, const GT *__restrict__ gdir,
-                                 double *__restrict__ lx, double *__restrict__ lm, uint32_t n) {
+                                 const double *__restrict__ scale, double *__restrict__ lx, double *__restrict__ lm,
+                                 uint32_t n) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     const uint32_t ui = sidx[j];
@@ -157,6 +158,10 @@ __global__ void k_adj_distribute(const double4 *__restrict__ body, const uint32_
         gm += an[3];
         p = oparent[p];
     }
+    if (scale) {  // the MIXED form's cotangents were scaled by a power of two
+        const double f = *scale;
+        gx *= f; gy *= f; gz *= f; gm *= f;
+    }
     lx[3 * (size_t)ui] += gx; lx[3 * (size_t)ui + 1] += gy; lx[3 * (size_t)ui + 2] += gz;
     lm[ui] += gm;
 }
@@ -171,26 +176,54 @@ cudaError_t launch_adj_pre(const double *lx, double *lv, void *lam, bool lam_dou
 
 cudaError_t launch_adj_distribute(const double4 *body, const uint32_t *sidx, const int32_t *leaf_oparent,
                                   const int32_t *oparent, const double4 *onode, const double *adj_node,
-                                  const double *adj_leaf, const void *gdir, bool gdir_double, double *lx, double *lm,
-                                  uint32_t n, cudaStream_t st) {
+                                  const double *adj_leaf, const void *gdir, bool gdir_double, const double *scale,
+                                  double *lx, double *lm, uint32_t n, cudaStream_t st) {
     const unsigned blocks = (n + 255) / 256;
     if (gdir_double)
         k_adj_distribute<double><<<blocks, 256, 0, st>>>(body, sidx, leaf_oparent, oparent, onode, adj_node, adj_leaf,
-                                                         (const double *)gdir, lx, lm, n);
+                                                         (const double *)gdir, scale, lx, lm, n);
     else
         k_adj_distribute<float><<<blocks, 256, 0, st>>>(body, sidx, leaf_oparent, oparent, onode, adj_node, adj_leaf,
-                                                        (const float *)gdir, lx, lm, n);
+                                                        (const float *)gdir, scale, lx, lm, n);
     return cudaGetLastError();
 }
 
-__global__ void k_double_to_float(const double *__restrict__ in, float *__restrict__ out, size_t count) {
-    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < count) out[i] = (float)in[i];
+// Largest |v| over count doubles, into *out (ordered bits of a non-negative double).
+__global__ void k_absmax(const double *__restrict__ v, size_t count, unsigned long long *out) {
+    __shared__ double s_w[32];
+    double m = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x)
+        m = fmax(m, fabs(v[i]));
+    m = warp_max(m);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) s_w[w] = m;
+    __syncthreads();
+    if (w == 0) {
+        m = lane < (int)(blockDim.x >> 5) ? s_w[lane] : 0.0;
+        m = warp_max(m);
+        if (lane == 0 && m > 0.0) atomic_max_nonneg(out, m);
+    }
 }
 
-cudaError_t launch_double_to_float(const double *in, float *out, size_t count, cudaStream_t st) {
-    if (!count) return cudaSuccess;
-    k_double_to_float<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(in, out, count);
+// out = in * 2^-e in FP32, where 2^e brings the largest |in| into [0.5, 1)
+// (e = 0 when it is zero or not finite); sc->lam_scale = 2^e.
+__global__ void k_scale_to_float(const double *__restrict__ in, float *__restrict__ out, size_t count,
+                                 DevScalars *sc) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const double mx = __longlong_as_double((long long)sc->lam_max_bits);
+    int e = 0;
+    if (mx > 0.0 && isfinite(mx)) frexp(mx, &e);
+    if (i == 0) sc->lam_scale = ldexp(1.0, e);
+    if (i < count) out[i] = (float)ldexp(in[i], -e);
+}
+
+cudaError_t launch_lam_to_float_scaled(const double *in, float *out, size_t count, DevScalars *sc, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(&sc->lam_max_bits, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    const size_t blocks = (count + 255) / 256;
+    k_absmax<<<(unsigned)std::max<size_t>(1, std::min<size_t>(blocks, 1184)), 256, 0, st>>>(in, count,
+                                                                                         &sc->lam_max_bits);
+    k_scale_to_float<<<(unsigned)std::max<size_t>(1, blocks), 256, 0, st>>>(in, out, count, sc);
     return cudaGetLastError();
 }
 

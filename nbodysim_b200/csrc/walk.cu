@@ -214,28 +214,52 @@ __device__ inline void force_near_f32(const double4 *nc, const uint32_t *nm, int
 template <bool kDamp, typename T>
 __device__ inline void pair_adjoint(T dx, T dy, T dz, T r2, T gm, T lax, T lay, T laz, T &vx, T &vy, T &vz,
                                     T &mterm) {
-    T inv, g, h;
-    if constexpr (sizeof(T) == 4) inv = rsqrt_ftz(r2);
-    else inv = 1.0 / sqrt(r2);
-    const T inv2 = inv * inv;
-    if constexpr (kDamp) {
-        const T r = r2 * inv;
-        T e;
-        if constexpr (sizeof(T) == 4) e = expf(-r);
-        else e = exp(-r);
-        const T den = r2 + e;
-        g = inv / den;
-        h = -(T(3) * r2 + e - r * e) * inv2 * inv / (den * den);
+    if constexpr (sizeof(T) == 4) {
+        // FP32: the same terms written with the unit offset u = d / r, so that no
+        // factor grows faster than the force itself (h alone, ~ r^-5, overflows
+        // FP32 below r ~ 2e-8): h s d = (h r^2) (u . la) u, G g s = G (g r) (u . la).
+        const float inv = rsqrt_ftz(r2);
+        const float ux = dx * inv, uy = dy * inv, uz = dz * inv;
+        const float sh = ux * lax + uy * lay + uz * laz;
+        float g, gr, hr2;
+        if constexpr (kDamp) {
+            const float r = r2 * inv;
+            const float e = expf(-r);
+            const float den = r2 + e;
+            g = inv / den;
+            gr = 1.f / den;
+            hr2 = -(3.f * r2 + e - r * e) * inv / (den * den);
+        } else {
+            gr = inv * inv;
+            g = gr * inv;
+            hr2 = -3.f * g;
+        }
+        const float c = hr2 * sh;
+        vx = gm * (g * lax + c * ux);
+        vy = gm * (g * lay + c * uy);
+        vz = gm * (g * laz + c * uz);
+        mterm = float(kG) * gr * sh;
     } else {
-        g = inv * inv2;
-        h = T(-3) * g * inv2;
+        const T inv = 1.0 / sqrt(r2);
+        const T inv2 = inv * inv;
+        T g, h;
+        if constexpr (kDamp) {
+            const T r = r2 * inv;
+            const T e = exp(-r);
+            const T den = r2 + e;
+            g = inv / den;
+            h = -(T(3) * r2 + e - r * e) * inv2 * inv / (den * den);
+        } else {
+            g = inv * inv2;
+            h = T(-3) * g * inv2;
+        }
+        const T s = dx * lax + dy * lay + dz * laz;
+        const T hs = h * s;
+        vx = gm * (g * lax + hs * dx);
+        vy = gm * (g * lay + hs * dy);
+        vz = gm * (g * laz + hs * dz);
+        mterm = T(kG) * g * s;
     }
-    const T s = dx * lax + dy * lay + dz * laz;
-    const T hs = h * s;
-    vx = gm * (g * lax + hs * dx);
-    vy = gm * (g * lay + hs * dy);
-    vz = gm * (g * laz + hs * dz);
-    mterm = T(kG) * g * s;
 }
 
 // Sums 32 per-lane values over the warp: lane l returns the sum over lanes of

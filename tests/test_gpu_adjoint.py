@@ -203,3 +203,26 @@ def test_backward_same_with_and_without_graphs(nb):
             grads.append(e.backward(2.0 * (xK - target) / n))
     for a, b in zip(*grads):
         assert np.abs(a - b).max() <= 1e-10 * np.abs(b).max()
+
+
+@pytest.mark.parametrize("precision", [1, 0])
+def test_backward_at_full_scale_independent_of_checkpoints(nb, precision):
+    """Config 4's size: the sphere of 65,536 particles, K = 256 steps. The
+    gradients with a checkpoint every 16 steps (and the octrees kept for the
+    reverse pass) equal those with a checkpoint every 64 steps; the forward
+    recomputation is bit-identical, so only the order of the reverse pass's
+    atomic sums differs."""
+    n, K = 65536, 256
+    pos, vel, mass = nb.generate(n, gen_type=1, size=512.0)
+    target = pos + np.random.default_rng(0xDEADBEEF).normal(0.0, 5.0, pos.shape)
+    grads = []
+    with nb.Engine(precision=precision, adaptive=0) as e:
+        for every in (16, 64):
+            e.set_particles(pos, vel, mass)
+            e.forward_checkpointed(K, every)
+            xK, _ = e.get_particles()
+            g = e.backward(2.0 * (xK - target) / n)
+            assert all(np.isfinite(x).all() for x in g)
+            grads.append(g)
+    for a, b in zip(grads[1], grads[0]):
+        assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max(), np.abs(a - b).max() / np.abs(b).max()
