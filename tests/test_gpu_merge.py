@@ -99,3 +99,15 @@ def test_merging_rejected_where_n_is_fixed(nb):
         e.set_particles(pos, vel, mass)
         e.compute_forces()  # forces only: nothing merges
         assert e.device_view().n == 300
+
+
+@pytest.mark.parametrize("gen_type,size,collide,rng,ms", [(0, 200.0, True, 1.0, 0.0), (1, 400.0, True, 0.5, 1.0)])
+def test_merging_matches_reference_at_60k(nb, ref, gen_type, size, collide, rng, ms):
+    """60,000 particles: hundreds of merges in one frame (pairs, chains and, in
+    the second case, minimum-size folds too), against the reference's frame."""
+    pos, vel, mass = nb.generate(60000, gen_type=gen_type, size=size)
+    wp, wv, _, wm = ref.frame_merging(pos, vel, mass, collide=collide, collision_range=rng, min_size=ms)
+    o = np.argsort(wm, kind="stable")
+    assert len(wm) < 60000 - 100
+    p, v, m, _ = run_gpu(nb, pos, vel, mass, nb.PRECISION_FP64, collide, rng, ms)
+    compare((p, v, m), (wp[o], wv[o], wm[o]), 1e-12)
