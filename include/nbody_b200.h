@@ -190,7 +190,11 @@ int nbody_get_diagnostics(nbody_ctx *ctx, nbody_diagnostics *out);
  * Reverse mode through the Barnes-Hut step with every step's opening decisions
  * and interaction lists frozen (no reference counterpart). Pair terms follow
  * the pair force's Jacobian; node terms flow through each node's centre of
- * mass and total mass to every particle inside it. */
+ * mass and total mass to every particle inside it. In the MIXED form the
+ * cotangents enter each FP32 pass scaled by a power of two that brings the
+ * largest into [0.5, 1), and the FP64 results are scaled back, so gradients far
+ * outside the FP32 range (they grow by many orders of magnitude through close
+ * encounters) stay finite. */
 
 /* Vector-Jacobian product of one force pass at the given state (host arrays):
  * dL_dpos = (da/dx)^T dL_dacc and dL_dmass = (da/dm)^T dL_dacc, n x 3 and n. */
