@@ -224,5 +224,8 @@ def test_backward_at_full_scale_independent_of_checkpoints(nb, precision):
             g = e.backward(2.0 * (xK - target) / n)
             assert all(np.isfinite(x).all() for x in g)
             grads.append(g)
+    # FP64 atomics in another order, and in the MIXED form a scale that may land on
+    # the other side of a power of two: differences at the rounding level of each form
+    tol = 1e-6 if precision == 1 else 1e-5
     for a, b in zip(grads[1], grads[0]):
-        assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max(), np.abs(a - b).max() / np.abs(b).max()
+        assert np.abs(a - b).max() <= tol * np.abs(b).max(), np.abs(a - b).max() / np.abs(b).max()
