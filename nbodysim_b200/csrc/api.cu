@@ -1360,12 +1360,12 @@ int nbody_backward(nbody_ctx *c, const double *dL_dpos, const double *dL_dvel, d
         for (int i = (int)len - 1; i >= 0; i--) {
             auto adj = [&, i]() -> int {
                 if (fp64) {
-                    NB_CUDA(launch_adj_pre(c->lx, c->lv, c->lam, true, c->p.dt, n, c->stream));
+                    NB_CUDA(launch_adj_pre(c->lx, c->lv, c->lam, c->p.dt, n, c->stream));
                     c->launches++;
                 } else {
                     // dL/da in FP64 (gdir is free until the walk), then scaled into FP32
                     double *lam_d = c->gdir;
-                    NB_CUDA(launch_adj_pre(c->lx, c->lv, lam_d, true, c->p.dt, n, c->stream));
+                    NB_CUDA(launch_adj_pre(c->lx, c->lv, lam_d, c->p.dt, n, c->stream));
                     NB_CUDA(launch_lam_to_float_scaled(lam_d, (float *)c->lam, N3, c->sc, c->stream));
                     c->launches += 3;
                 }

@@ -118,14 +118,13 @@ __global__ void k_acc_to_double(const float *__restrict__ in, double *__restrict
 // Reverse of particle::update (src/particle.cpp:66-74): with x' = x + v' dt and
 // v' = v + a dt, the cotangents of step k follow from those of step k+1 as
 //   mu = lv' + lx' dt;  lv = mu;  la = mu dt;  lx = lx' + (dF/dx)^T la.
-template <typename LT>
-__global__ void k_adj_pre(const double *__restrict__ lx, double *__restrict__ lv, LT *__restrict__ lam, double dt,
+__global__ void k_adj_pre(const double *__restrict__ lx, double *__restrict__ lv, double *__restrict__ lam, double dt,
                           uint32_t n) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= 3 * (size_t)n) return;
     const double mu = lv[i] + lx[i] * dt;
     lv[i] = mu;
-    lam[i] = (LT)(mu * dt);
+    lam[i] = mu * dt;
 }
 
 // Node cotangents -> particles. A particle j inside node n (its own leaf and
@@ -166,11 +165,9 @@ __global__ void k_adj_distribute(const double4 *__restrict__ body, const uint32_
     lm[ui] += gm;
 }
 
-cudaError_t launch_adj_pre(const double *lx, double *lv, void *lam, bool lam_double, double dt, uint32_t n,
-                           cudaStream_t st) {
+cudaError_t launch_adj_pre(const double *lx, double *lv, double *lam, double dt, uint32_t n, cudaStream_t st) {
     const unsigned blocks = (unsigned)((3 * (size_t)n + 255) / 256);
-    if (lam_double) k_adj_pre<double><<<blocks, 256, 0, st>>>(lx, lv, (double *)lam, dt, n);
-    else k_adj_pre<float><<<blocks, 256, 0, st>>>(lx, lv, (float *)lam, dt, n);
+    k_adj_pre<<<blocks, 256, 0, st>>>(lx, lv, lam, dt, n);
     return cudaGetLastError();
 }
 

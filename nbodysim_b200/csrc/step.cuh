@@ -25,8 +25,8 @@ cudaError_t launch_acc_to_double(const float *in, double *out, size_t count, cud
 // largest into [0.5, 1) (the FP32 range would not hold them through many reverse
 // steps); the factor back is left in sc->lam_scale.
 cudaError_t launch_lam_to_float_scaled(const double *in, float *out, size_t count, DevScalars *sc, cudaStream_t st);
-cudaError_t launch_adj_pre(const double *lx, double *lv, void *lam, bool lam_double, double dt, uint32_t n,
-                           cudaStream_t st);
+// mu = lv + lx dt -> lv; dL/da = mu dt -> lam (FP64)
+cudaError_t launch_adj_pre(const double *lx, double *lv, double *lam, double dt, uint32_t n, cudaStream_t st);
 cudaError_t launch_adj_distribute(const double4 *body, const uint32_t *sidx, const int32_t *leaf_oparent,
                                   const int32_t *oparent, const double4 *onode, const double *adj_node,
                                   const double *adj_leaf, const void *gdir, bool gdir_double, const double *scale,
