@@ -140,3 +140,22 @@ def test_ensemble_at_full_scale(nb, orc):
             if k < 2:
                 _, rc = orc.forces(p, m, 0.5)
                 assert np.array_equal(cnt, rc), s
+
+
+def test_ensemble_through_step_host(nb):
+    """nbody_step_host on an ensemble large enough for the overlapped uploads
+    (masses and velocities on a second stream; the per-system root cubes wait
+    for the masses): the same as the resident steps, bit for bit."""
+    counts = [30000, 25000, 20000]
+    parts, pos, vel, mass = make_systems(nb, counts, seed=11)
+    with nb.Engine() as e:
+        e.set_systems(counts)
+        e.set_particles(pos, vel, mass)
+        e.step(2)
+        p1, v1 = e.get_particles()
+    with nb.Engine() as e:
+        e.set_systems(counts)
+        p2, v2 = pos.copy(), vel.copy()
+        e.step_host(p2, v2, mass, 1)
+        e.step_host(p2, v2, mass, 1)
+    assert np.array_equal(p1, p2) and np.array_equal(v1, v2)
