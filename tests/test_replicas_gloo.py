@@ -3,7 +3,6 @@ CPU with gloo: the job's time is the slowest rank's and the work is the sum."""
 import os
 import socket
 
-import pytest
 import torch.multiprocessing as mp
 
 
