@@ -303,7 +303,7 @@ inline unsigned blocks_for(uint64_t n, unsigned t) { return (unsigned)((n + t - 
 }  // namespace
 
 cudaError_t merge_begin(const MergeBufs &m, uint32_t n, cudaStream_t st, unsigned *launches) {
-    k_merge_init<<<blocks_for(n > kMcCount ? n : kMcCount, 256), 256, 0, st>>>(m, n);
+    k_merge_init<<<blocks_for(std::max<uint32_t>(n, kMcCount), 256), 256, 0, st>>>(m, n);
     *launches += 1;
     return cudaGetLastError();
 }
