@@ -24,6 +24,20 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libnbref.so")
 REF_LIB_F32 = os.path.join(HERE, "_ref", "libnbref_f32.so")
+# the DOUBLE build with the reference's release flags (-march=x86-64-v3 for
+# -march=native): the timed CPU baseline, not a parity checker
+REF_LIB_REL = os.path.join(HERE, "_ref", "libnbref_rel.so")
+
+
+def release_build_usable() -> bool:
+    """The release build needs AVX2, FMA and BMI2 on the host running it."""
+    if not os.path.exists(REF_LIB_REL):
+        return False
+    try:
+        flags = open("/proc/cpuinfo").read().split()
+    except OSError:
+        return False
+    return all(f in flags for f in ("avx2", "fma", "bmi2"))
 ORACLE_LIB = os.path.join(HERE, "lib", "libbh_oracle.so")
 
 CUBE, SPHERE, SHELL = 0, 1, 2
@@ -85,7 +99,7 @@ def _c64(a):
 
 
 class Reference:
-    """The reference's own CPU code (DOUBLE build by default)."""
+    """The reference's own CPU code (DOUBLE build by default; REF_LIB_F32 is its FLOAT build)."""
 
     def __init__(self, path: str = REF_LIB):
         if not os.path.exists(path):
@@ -187,8 +201,12 @@ class Oracle:
         L = self.lib
         L.bho_generate.argtypes = [C.POINTER(_CGen), C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
         L.bho_root_cube.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.bho_root_cube_f32.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
         L.bho_build.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p]
         L.bho_build.restype = C.c_void_p
+        L.bho_build_f32.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p]
+        L.bho_build_f32.restype = C.c_void_p
+        L.bho_update_f32.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]
         L.bho_free.argtypes = [C.c_void_p]
         L.bho_node_count.argtypes = [C.c_void_p]
         L.bho_node_count.restype = C.c_int64
@@ -198,6 +216,7 @@ class Oracle:
         L.bho_update.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]
         L.bho_run_frames.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int,
                                      C.c_double, C.c_int, C.c_uint32, C.c_void_p]
+        L.bho_run_frames_f32.argtypes = L.bho_run_frames.argtypes
         L.bho_direct.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_uint32,
                                  C.c_int, C.c_void_p]
         L.bho_tree_nodes.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -210,17 +229,25 @@ class Oracle:
             raise ValueError("invalid generation parameters")
         return pos, vel, mass
 
-    def root_cube(self, pos):
+    def root_cube(self, pos, single=False):
+        """Root cube; single=True: as the reference's FLOAT build computes it."""
         pos = _c64(pos)
         c = np.zeros(3); s = np.zeros(1)
-        self.lib.bho_root_cube(len(pos), pos.ctypes.data, c.ctypes.data, s.ctypes.data)
+        fn = self.lib.bho_root_cube_f32 if single else self.lib.bho_root_cube
+        fn(len(pos), pos.ctypes.data, c.ctypes.data, s.ctypes.data)
         return c, float(s[0])
 
-    def forces(self, pos, mass, theta=0.5, damping=False, threads=None, sample=None, with_stats=False):
-        """Accelerations (and per-particle accepted-node counts) from the BH walk."""
+    def _build(self, pos, mass, single):
+        fn = self.lib.bho_build_f32 if single else self.lib.bho_build
+        return fn(len(mass), pos.ctypes.data, mass.ctypes.data)
+
+    def forces(self, pos, mass, theta=0.5, damping=False, threads=None, sample=None, with_stats=False,
+               single=False):
+        """Accelerations (and per-particle accepted-node counts) from the BH walk.
+        single=True follows the reference's FLOAT build (results are floats)."""
         pos = _c64(pos); mass = _c64(mass); n = len(mass)
         threads = threads or os.cpu_count() or 1
-        t = self.lib.bho_build(n, pos.ctypes.data, mass.ctypes.data)
+        t = self._build(pos, mass, single)
         if not t and n:
             raise RuntimeError("oracle tree build failed (coincident particles or out of memory)")
         try:
@@ -245,9 +272,9 @@ class Oracle:
             return acc, cnt, stats
         return acc, cnt
 
-    def tree_nodes(self, pos, mass):
+    def tree_nodes(self, pos, mass, single=False):
         pos = _c64(pos); mass = _c64(mass); n = len(mass)
-        t = self.lib.bho_build(n, pos.ctypes.data, mass.ctypes.data)
+        t = self._build(pos, mass, single)
         cap = 4 * n + 8
         lv = np.zeros(cap, np.int32); ct = np.zeros(cap, np.int32); mi = np.zeros(cap, np.int32)
         nm = np.zeros(cap); com = np.zeros((cap, 3)); sd = np.zeros(cap)
@@ -260,16 +287,21 @@ class Oracle:
         return dict(level=lv[:k], count=ct[:k], min_index=mi[:k], mass=nm[:k], com=com[:k],
                     side=sd[:k], depth=depth)
 
-    def update(self, pos, vel, acc, dt):
+    def update(self, pos, vel, acc, dt, single=False):
         pos = _c64(pos).copy(); vel = _c64(vel).copy(); acc = _c64(acc)
-        self.lib.bho_update(len(pos), pos.ctypes.data, vel.ctypes.data, acc.ctypes.data, dt)
+        fn = self.lib.bho_update_f32 if single else self.lib.bho_update
+        fn(len(pos), pos.ctypes.data, vel.ctypes.data, acc.ctypes.data, dt)
         return pos, vel
 
     def run_frames(self, pos, vel, mass, frames, theta=0.5, damping=False, dt=0.0333, threads=None,
-                   keep_frames=False):
+                   keep_frames=False, single=False):
         pos = _c64(pos).copy(); vel = _c64(vel).copy(); mass = _c64(mass); n = len(mass)
+        if single:
+            pos = pos.astype(np.float32).astype(np.float64)
+            vel = vel.astype(np.float32).astype(np.float64)
         out = np.zeros((frames, n, 3)) if keep_frames else None
-        rc = self.lib.bho_run_frames(n, pos.ctypes.data, vel.ctypes.data, mass.ctypes.data, theta,
+        fn = self.lib.bho_run_frames_f32 if single else self.lib.bho_run_frames
+        rc = fn(n, pos.ctypes.data, vel.ctypes.data, mass.ctypes.data, theta,
                                      int(damping), dt, threads or os.cpu_count() or 1, frames,
                                      out.ctypes.data if out is not None else None)
         if rc:

@@ -166,7 +166,19 @@ struct bho_tree {
     bho_node *nodes;
     int64_t count, cap;
     int depth;
+    int single; /* the reference's FLOAT build: every value below is a float */
 };
+
+/* In a FLOAT tree positions and masses enter as floats, as the reference
+ * harness converts them (datatype). */
+static double in_pos(const bho_tree *t, size_t i, int k) {
+    const double v = t->pos[3 * i + k];
+    return t->single ? (double)(float)v : v;
+}
+static double in_mass(const bho_tree *t, size_t i) {
+    const double v = t->mass[i];
+    return t->single ? (double)(float)v : v;
+}
 
 /* Root cube, src/main.cpp:889-920: bbox midpoint; side = largest extent + 2,
  * a tie for the largest extent falls through to the z extent. */
@@ -184,6 +196,27 @@ void bho_root_cube(uint32_t n, const double *pos, double *center, double *side) 
     if (ex > ey && ex > ez) *side = ex + 2.0;
     else if (ey > ex && ey > ez) *side = ey + 2.0;
     else *side = ez + 2.0;
+}
+
+/* The same in the FLOAT build (src/main.cpp:889-920 with datatype float): float
+ * extrema; center = float(min + max) / 2.0 (exact halving, back to float);
+ * side = float(float(max - min) + 2.0); the extent comparisons in float. */
+void bho_root_cube_f32(uint32_t n, const double *pos, double *center, double *side) {
+    float mn[3] = {3.40282347e38f, 3.40282347e38f, 3.40282347e38f};
+    float mx[3] = {-3.40282347e38f, -3.40282347e38f, -3.40282347e38f};
+    for (uint32_t i = 0; i < n; i++)
+        for (int k = 0; k < 3; k++) {
+            float v = (float)pos[3 * i + k];
+            if (v < mn[k]) mn[k] = v;
+            if (v > mx[k]) mx[k] = v;
+        }
+    for (int k = 0; k < 3; k++) center[k] = (double)(float)((double)(mn[k] + mx[k]) / 2.0);
+    float ex = mx[0] - mn[0], ey = mx[1] - mn[1], ez = mx[2] - mn[2];
+    float s;
+    if (ex > ey && ex > ez) s = (float)((double)ex + 2.0);
+    else if (ey > ex && ey > ez) s = (float)((double)ey + 2.0);
+    else s = (float)((double)ez + 2.0);
+    *side = (double)s;
 }
 
 static int32_t new_node(bho_tree *t, const double *center, double side) {
@@ -204,22 +237,30 @@ static int32_t new_node(bho_tree *t, const double *center, double side) {
 }
 
 /* Octant: x bit 1, y bit 2, z bit 4, strict '>' (src/octree.cpp:153-165). */
-static int octant(const double *x, const double *c) {
+static int octant(const bho_tree *t, int32_t par, const double *c) {
     int i = 0;
-    if (x[0] > c[0]) i += 1;
-    if (x[1] > c[1]) i += 2;
-    if (x[2] > c[2]) i += 4;
+    if (in_pos(t, (size_t)par, 0) > c[0]) i += 1;
+    if (in_pos(t, (size_t)par, 1) > c[1]) i += 2;
+    if (in_pos(t, (size_t)par, 2) > c[2]) i += 4;
     return i;
 }
 
 /* allocate_child, src/octree.cpp:54-85: center += (+-half/2) per axis. */
 static int32_t alloc_child(bho_tree *t, int32_t node, int i) {
-    double half = t->nodes[node].side / 2;
     int sx = (i & 1) ? 1 : -1, sy = (i & 2) ? 1 : -1, sz = (i & 4) ? 1 : -1;
-    double c[3];
-    c[0] = t->nodes[node].center[0] + sx * half / 2;
-    c[1] = t->nodes[node].center[1] + sy * half / 2;
-    c[2] = t->nodes[node].center[2] + sz * half / 2;
+    double c[3], half;
+    if (t->single) {
+        float h = (float)t->nodes[node].side / 2;
+        c[0] = (float)t->nodes[node].center[0] + sx * h / 2;
+        c[1] = (float)t->nodes[node].center[1] + sy * h / 2;
+        c[2] = (float)t->nodes[node].center[2] + sz * h / 2;
+        half = h;
+    } else {
+        half = t->nodes[node].side / 2;
+        c[0] = t->nodes[node].center[0] + sx * half / 2;
+        c[1] = t->nodes[node].center[1] + sy * half / 2;
+        c[2] = t->nodes[node].center[2] + sz * half / 2;
+    }
     int32_t k = new_node(t, c, half);
     if (k >= 0) t->nodes[node].child[i] = k;
     return k;
@@ -238,13 +279,13 @@ static int add_particle(bho_tree *t, int32_t node, int32_t par, int level) {
             for (int k = 0; k < 8; k++)
                 if (d->child[k] >= 0) { leaf = 0; break; }
             if (leaf) { d->p = par; return 0; }
-            int i = octant(&t->pos[3 * (size_t)par], d->center);
+            int i = octant(t, par, d->center);
             if (d->child[i] < 0 && alloc_child(t, node, i) < 0) return -1;
             node = t->nodes[node].child[i];
             level++;
         } else {
             int32_t q = d->p;
-            int i = octant(&t->pos[3 * (size_t)q], d->center);
+            int i = octant(t, q, d->center);
             int32_t c = t->nodes[node].child[i];
             if (c < 0 && (c = alloc_child(t, node, i)) < 0) return -1;
             if (level + 1 > t->depth) t->depth = level + 1;
@@ -258,18 +299,38 @@ static int add_particle(bho_tree *t, int32_t node, int32_t par, int level) {
 static void mass_com(bho_tree *t, int32_t node) {
     bho_node *d = &t->nodes[node];
     if (d->p >= 0) {
-        d->mass = t->mass[d->p];
-        for (int k = 0; k < 3; k++) d->com[k] = t->pos[3 * (size_t)d->p + k];
+        d->mass = in_mass(t, (size_t)d->p);
+        for (int k = 0; k < 3; k++) d->com[k] = in_pos(t, (size_t)d->p, k);
+        return;
+    }
+    for (int i = 0; i < 8; i++) {
+        int32_t c = t->nodes[node].child[i];
+        if (c >= 0) mass_com(t, c);
+    }
+    d = &t->nodes[node];
+    if (t->single) {
+        /* FLOAT build: float sums in child order, float products and quotient */
+        float m = 0;
+        for (int i = 0; i < 8; i++)
+            if (d->child[i] >= 0) m += (float)t->nodes[d->child[i]].mass;
+        d->mass = m;
+        if (m == 0) { d->com[0] = d->com[1] = d->com[2] = 0; return; }
+        float s[3] = {0, 0, 0};
+        for (int i = 0; i < 8; i++) {
+            int32_t c = d->child[i];
+            if (c < 0) continue;
+            float cm = (float)t->nodes[c].mass;
+            for (int k = 0; k < 3; k++) {
+                float w = (float)t->nodes[c].com[k] * cm;
+                s[k] += w;
+            }
+        }
+        for (int k = 0; k < 3; k++) d->com[k] = s[k] / m;
         return;
     }
     double m = 0;
-    for (int i = 0; i < 8; i++) {
-        int32_t c = t->nodes[node].child[i];
-        if (c < 0) continue;
-        mass_com(t, c);
-        m += t->nodes[c].mass;
-    }
-    d = &t->nodes[node];
+    for (int i = 0; i < 8; i++)
+        if (d->child[i] >= 0) m += t->nodes[d->child[i]].mass;
     d->mass = m;
     if (m == 0) { d->com[0] = d->com[1] = d->com[2] = 0; return; }
     double s[3] = {0, 0, 0};
@@ -284,18 +345,23 @@ static void mass_com(bho_tree *t, int32_t node) {
     d->com[0] = s[0] / m; d->com[1] = s[1] / m; d->com[2] = s[2] / m;
 }
 
-bho_tree *bho_build(uint32_t n, const double *pos, const double *mass) {
+static bho_tree *build(uint32_t n, const double *pos, const double *mass, int single) {
     bho_tree *t = (bho_tree *)calloc(1, sizeof(bho_tree));
     if (!t) return NULL;
-    t->n = n; t->pos = pos; t->mass = mass;
+    t->n = n; t->pos = pos; t->mass = mass; t->single = single;
     double c[3], side;
-    bho_root_cube(n, pos, c, &side);
+    if (single) bho_root_cube_f32(n, pos, c, &side);
+    else bho_root_cube(n, pos, c, &side);
     if (new_node(t, c, side) < 0) { bho_free(t); return NULL; }
     for (uint32_t i = 0; i < n; i++)
         if (add_particle(t, 0, (int32_t)i, 0) != 0) { bho_free(t); return NULL; }
     if (n > 0) mass_com(t, 0);
     return t;
 }
+
+bho_tree *bho_build_f32(uint32_t n, const double *pos, const double *mass) { return build(n, pos, mass, 1); }
+
+bho_tree *bho_build(uint32_t n, const double *pos, const double *mass) { return build(n, pos, mass, 0); }
 
 void bho_free(bho_tree *t) {
     if (!t) return;
@@ -326,6 +392,41 @@ static void gravity(const double *com, double nmass, const double *x, int dampin
     out[0] = a[0]; out[1] = a[1]; out[2] = a[2];
 }
 
+/* The FLOAT build's distance() and gravity() (src/vector.cpp:99-109,
+ * src/main.cpp:306-333 with datatype float): float differences; pow(float, 2)
+ * promotes to double, so the squares and their sum are double, and sqrt's
+ * double result is rounded back to float; pow(magnitude, -2) is taken in
+ * double and rounded to float; exp() of a float is expf; G is rounded to float
+ * by operator*=(const datatype &). */
+static float magnitude_f32(float x, float y, float z) {
+    return (float)sqrt(pow((double)x, 2) + pow((double)y, 2) + pow((double)z, 2));
+}
+
+static float distance_f32(const double *a, const double *b) {
+    float dx = (float)a[0] - (float)b[0], dy = (float)a[1] - (float)b[1], dz = (float)a[2] - (float)b[2];
+    return magnitude_f32(dx, dy, dz);
+}
+
+static void gravity_f32(const double *com, double nmass, const double *x, int damping, float *out) {
+    float a[3] = {(float)com[0] - (float)x[0], (float)com[1] - (float)x[1], (float)com[2] - (float)x[2]};
+    float r_sq;
+    if (!damping) {
+        r_sq = (float)pow((double)magnitude_f32(a[0], a[1], a[2]), -2);
+    } else {
+        float mg = magnitude_f32(a[0], a[1], a[2]);
+        r_sq = (float)(1.0 / (pow((double)mg, 2) + (double)expf(-1 * mg)));
+    }
+    float mag = magnitude_f32(a[0], a[1], a[2]);
+    const float m = (float)nmass, g = (float)BHO_G;
+    for (int k = 0; k < 3; k++) {
+        a[k] /= mag;
+        a[k] *= m;
+        a[k] *= g;
+        a[k] *= r_sq;
+        out[k] = a[k];
+    }
+}
+
 typedef struct {
     const bho_tree *t;
     double theta;
@@ -348,23 +449,35 @@ static void *walk_range(void *arg) {
     if (!queue) { j->err = -1; return NULL; }
     for (uint32_t s = j->begin; s < j->end; s++) {
         uint32_t i = j->sample ? j->sample[s] : s;
-        const double *x = &t->pos[3 * (size_t)i];
+        const double x[3] = {in_pos(t, i, 0), in_pos(t, i, 1), in_pos(t, i, 2)};
         double acc[3] = {0, 0, 0};
         uint32_t cnt = 0;
         int64_t head = 0, tail = 0;
         queue[tail++] = 0;
+        float facc[3] = {0, 0, 0};
+        const float ftheta = (float)j->theta;
         while (head < tail) {
             const bho_node *d = &t->nodes[queue[head++]];
-            if (d->side / distance3(d->com, x) > j->theta && d->p < 0) {
+            int open;
+            if (t->single) open = (float)d->side / distance_f32(d->com, x) > ftheta && d->p < 0;
+            else open = d->side / distance3(d->com, x) > j->theta && d->p < 0;
+            if (open) {
                 for (int k = 0; k < 8; k++)
                     if (d->child[k] >= 0) queue[tail++] = d->child[k];
             } else if (d->p != (int32_t)i) {
-                double g[3];
-                gravity(d->com, d->mass, x, j->damping, g);
-                acc[0] += g[0]; acc[1] += g[1]; acc[2] += g[2];
+                if (t->single) {
+                    float g[3];
+                    gravity_f32(d->com, d->mass, x, j->damping, g);
+                    facc[0] += g[0]; facc[1] += g[1]; facc[2] += g[2];
+                } else {
+                    double g[3];
+                    gravity(d->com, d->mass, x, j->damping, g);
+                    acc[0] += g[0]; acc[1] += g[1]; acc[2] += g[2];
+                }
                 cnt++;
             }
         }
+        if (t->single) { acc[0] = facc[0]; acc[1] = facc[1]; acc[2] = facc[2]; }
         j->acc[3 * (size_t)s] = acc[0];
         j->acc[3 * (size_t)s + 1] = acc[1];
         j->acc[3 * (size_t)s + 2] = acc[2];
@@ -411,21 +524,44 @@ void bho_update(uint32_t n, double *pos, double *vel, const double *acc, double 
         }
 }
 
-int bho_run_frames(uint32_t n, double *pos, double *vel, const double *mass, double theta,
-                   int damping, double dt, int threads, uint32_t frames, double *frames_out) {
+/* The same in the FLOAT build: temp = a * dt; v += temp; temp = v * dt; x += temp, in float. */
+void bho_update_f32(uint32_t n, double *pos, double *vel, const double *acc, double dt) {
+    const float fdt = (float)dt;
+    for (size_t i = 0; i < (size_t)n; i++)
+        for (int k = 0; k < 3; k++) {
+            float v = (float)vel[3 * i + k] + (float)acc[3 * i + k] * fdt;
+            float x = (float)pos[3 * i + k] + v * fdt;
+            vel[3 * i + k] = v;
+            pos[3 * i + k] = x;
+        }
+}
+
+static int run_frames(uint32_t n, double *pos, double *vel, const double *mass, double theta, int damping,
+                      double dt, int threads, uint32_t frames, double *frames_out, int single) {
     double *acc = (double *)malloc((size_t)n * 3 * sizeof(double) + 8);
     if (!acc) return -1;
     for (uint32_t f = 0; f < frames; f++) {
-        bho_tree *t = bho_build(n, pos, mass);
+        bho_tree *t = build(n, pos, mass, single);
         if (!t) { free(acc); return -2; }
         int rc = bho_forces(t, theta, damping, threads, NULL, 0, acc, NULL);
         bho_free(t);
         if (rc) { free(acc); return rc; }
-        bho_update(n, pos, vel, acc, dt);
+        if (single) bho_update_f32(n, pos, vel, acc, dt);
+        else bho_update(n, pos, vel, acc, dt);
         if (frames_out) memcpy(frames_out + (size_t)f * n * 3, pos, (size_t)n * 3 * sizeof(double));
     }
     free(acc);
     return 0;
+}
+
+int bho_run_frames(uint32_t n, double *pos, double *vel, const double *mass, double theta,
+                   int damping, double dt, int threads, uint32_t frames, double *frames_out) {
+    return run_frames(n, pos, vel, mass, theta, damping, dt, threads, frames, frames_out, 0);
+}
+
+int bho_run_frames_f32(uint32_t n, double *pos, double *vel, const double *mass, double theta,
+                       int damping, double dt, int threads, uint32_t frames, double *frames_out) {
+    return run_frames(n, pos, vel, mass, theta, damping, dt, threads, frames, frames_out, 1);
 }
 
 /* ------------------------------------------------------------- direct sum */

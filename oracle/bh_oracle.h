@@ -12,7 +12,9 @@
  *   bho_mass_com     src/octree.cpp:203-221, 252-278
  *   bho_forces       src/main.cpp:306-333 (gravity), 335-421 (BFS walk)
  *   bho_update       src/particle.cpp:66-74, src/main.cpp:929-933
- * plus an FP64 direct-sum oracle (no reference counterpart).
+ * plus an FP64 direct-sum oracle (no reference counterpart). The _f32 entry
+ * points restate the same path as the reference's FLOAT build (-DFLOAT, the
+ * build its makefile ships) computes it, bit-identical to that build.
  * Arrays are AoS: pos[3*i+k], k = x,y,z.
  */
 #ifndef BH_ORACLE_H
@@ -41,9 +43,17 @@ int bho_generate(const bho_gen_params *g, uint32_t n, double *pos, double *vel, 
 /* Root cube (src/main.cpp:898-920): center[3], side. */
 void bho_root_cube(uint32_t n, const double *pos, double *center, double *side);
 
+/* The same in the reference's FLOAT build (float extrema, float center and side). */
+void bho_root_cube_f32(uint32_t n, const double *pos, double *center, double *side);
+
 /* Pointer octree with one particle per leaf; NULL on allocation failure or when
  * two particles coincide (the reference recurses without bound there). */
 bho_tree *bho_build(uint32_t n, const double *pos, const double *mass);
+/* The same tree as the reference's FLOAT build makes it: positions and masses
+ * rounded to float, child centres, masses and centres of mass in float
+ * arithmetic; bho_forces on such a tree follows the FLOAT build's opening test
+ * and gravity (results are floats widened to double). */
+bho_tree *bho_build_f32(uint32_t n, const double *pos, const double *mass);
 void bho_free(bho_tree *t);
 int64_t bho_node_count(const bho_tree *t);
 int bho_depth(const bho_tree *t);
@@ -57,9 +67,15 @@ int bho_forces(const bho_tree *t, double theta, int damping, int threads,
 /* Semi-implicit Euler, in place: v += a dt; x += v dt. */
 void bho_update(uint32_t n, double *pos, double *vel, const double *acc, double dt);
 
+/* The FLOAT build's update (float arithmetic); pos/vel hold floats afterwards. */
+void bho_update_f32(uint32_t n, double *pos, double *vel, const double *acc, double dt);
+
 /* Full frames: build -> mass/COM -> walk -> update, `frames` times. */
 int bho_run_frames(uint32_t n, double *pos, double *vel, const double *mass, double theta,
                    int damping, double dt, int threads, uint32_t frames, double *frames_out);
+/* The same frame loop in the FLOAT build (float tree, walk, gravity and update). */
+int bho_run_frames_f32(uint32_t n, double *pos, double *vel, const double *mass, double theta,
+                       int damping, double dt, int threads, uint32_t frames, double *frames_out);
 
 /* FP64 direct sum for the listed targets against all n sources (compensated
  * summation). acc_out: m x 3. */

@@ -1,11 +1,12 @@
 """Generates the golden fixtures in this folder from the reference's own code.
 
 Runs only where the reference tree is present and ``make -C oracle ref`` has
-built ``oracle/_ref/libnbref.so`` (fosted3/nbodysim's src/main.cpp, octree.cpp,
-particle.cpp, vector.cpp compiled unmodified, DOUBLE build). The outputs are
-small ``.npz`` files that pin the oracle (``oracle/bh_oracle.c``) where the
-reference is absent. Usage: ``python tests/golden/make_golden.py`` (all), or
-``python tests/golden/make_golden.py merging`` (the merging fixture only).
+built ``oracle/_ref/libnbref.so`` and ``libnbref_f32.so`` (fosted3/nbodysim's
+src/main.cpp, octree.cpp, particle.cpp, vector.cpp compiled unmodified, DOUBLE
+and FLOAT builds). The outputs are small ``.npz`` files that pin the oracle
+(``oracle/bh_oracle.c``) where the reference is absent. Usage:
+``python tests/golden/make_golden.py`` (all), or with ``merging`` or ``float``
+for one fixture only.
 """
 from __future__ import annotations
 
@@ -25,6 +26,53 @@ def lattice(k: int, step: float = 1.0):
     r = (np.arange(k) - (k - 1) / 2.0) * step
     g = np.stack(np.meshgrid(r, r, r, indexing="ij"), -1).reshape(-1, 3)
     return np.ascontiguousarray(g), np.full(len(g), 1e10)
+
+
+def split_plane_set(seed: int = 0, n: int = 2000):
+    """Float positions in an asymmetric box, so that the sum of the extrema on
+    some axis needs more bits than a float holds: the FLOAT build's root centre
+    (float(lo + hi) / 2) then lies an ulp above the DOUBLE build's, and 24
+    particles placed exactly on it fall into the upper root octant in the DOUBLE
+    build and the lower one in the FLOAT build. Over a thousand particles then
+    accept different nodes in the two builds."""
+    rng = np.random.default_rng(seed)
+    pos = rng.uniform(0.2, 99.0, (n, 3)).astype(np.float32)
+    pos[0] = np.float32([0.1, 0.15, 0.13])
+    pos[1] = np.float32([100.0, 99.7, 99.9])
+    lo, hi = pos.min(0), pos.max(0)
+    cd = (lo.astype(np.float64) + hi.astype(np.float64)) / 2.0
+    cf = ((lo + hi).astype(np.float64) / 2.0).astype(np.float32)
+    extra = []
+    for k in range(3):
+        if float(cf[k]) > cd[k]:
+            for _ in range(24):
+                p = rng.uniform(5.0, 95.0, 3).astype(np.float32)
+                p[k] = cf[k]
+                extra.append(p)
+    if extra:
+        pos = np.concatenate([pos, np.array(extra, np.float32)])
+    mass = rng.uniform(5e10, 5e11, len(pos)).astype(np.float32)
+    return np.ascontiguousarray(pos, np.float64), mass.astype(np.float64)
+
+
+def float_build() -> None:
+    """The FLOAT build (-DFLOAT, the reference makefile's build): forces on the
+    split-plane set and on the default cube, tree records, three frames."""
+    R = O.Reference(O.REF_LIB_F32)
+    assert R.datatype_bytes == 4
+    pos, mass = split_plane_set(0)
+    out = dict(split_pos=pos, split_mass=mass)
+    for th in (0.3, 0.5, 0.7):
+        out[f"split_acc_{th}"] = R.forces(pos, mass, th)[0]
+    out["split_acc_damped_0.5"] = R.forces(pos, mass, 0.5, damping=True)[0]
+    t = R.tree_nodes(pos, mass)
+    out.update({"split_node_" + k: np.asarray(v) for k, v in t.items()})
+    cpos, cvel, cmass = R.generate(O.GenParams(), 512)
+    out.update(cube_pos=cpos, cube_mass=cmass, cube_acc_0_5=R.forces(cpos, cmass, 0.5)[0])
+    fpos, fvel, fmass = R.generate(O.GenParams(min_vel=0.5, max_vel=2.0), 256)
+    _, _, frames = R.run_frames(fpos, fvel, fmass, 3, keep_frames=True)
+    out.update(frames_pos=fpos, frames_vel=fvel, frames_mass=fmass, frames=frames)
+    np.savez_compressed(os.path.join(HERE, "forces_float.npz"), **out)
 
 
 MERGE_CASES = (  # name, collide, collision_range, min_size
@@ -53,7 +101,11 @@ def main() -> None:
     if sys.argv[1:] == ["merging"]:
         merging(R)
         return
+    if sys.argv[1:] == ["float"]:
+        float_build()
+        return
     merging(R)
+    float_build()
     out = {}
     # seeded initial conditions: 64 particles per gen type x mass distribution
     for gt in (O.CUBE, O.SPHERE, O.SHELL):

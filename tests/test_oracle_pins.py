@@ -134,3 +134,63 @@ def test_reference_merging_hand_cases(ref):
     assert np.array_equal(v[k], vm) and np.array_equal(p[k], pm + vm * dt)
     _, _, _, m = ref.frame_merging(pos, vel, mass, collide=True, collision_range=0.05)
     assert len(m) == 3
+
+
+# ---- the reference's FLOAT build (-DFLOAT, the build its makefile ships) ----
+
+def test_float_build_forces_golden(orc, golden):
+    """Split-plane set (particles on the FLOAT build's root centre, which lies an
+    ulp from the DOUBLE build's) and the default cube: the oracle's FLOAT path
+    equals the FLOAT reference bit for bit, and its accepted nodes differ from
+    the DOUBLE build's for over a thousand particles."""
+    g = golden("forces_float.npz")
+    pos, mass = g["split_pos"], g["split_mass"]
+    for th in (0.3, 0.5, 0.7):
+        acc, cnt = orc.forces(pos, mass, th, single=True)
+        assert np.array_equal(acc, g[f"split_acc_{th}"]), th
+    acc, cnt32 = orc.forces(pos, mass, 0.5, damping=True, single=True)
+    assert np.array_equal(acc, g["split_acc_damped_0.5"])
+    _, cnt64 = orc.forces(pos, mass, 0.5)
+    _, cnt32 = orc.forces(pos, mass, 0.5, single=True)
+    assert (cnt32 != cnt64).sum() > 500
+    acc, _ = orc.forces(g["cube_pos"], g["cube_mass"], 0.5, single=True)
+    assert np.array_equal(acc, g["cube_acc_0_5"])
+
+
+def test_float_build_tree_and_frames_golden(orc, golden):
+    g = golden("forces_float.npz")
+    t = orc.tree_nodes(g["split_pos"], g["split_mass"], single=True)
+    for k in ("level", "count", "min_index", "mass", "com", "side"):
+        assert np.array_equal(t[k], g["split_node_" + k]), k
+    _, _, frames = orc.run_frames(g["frames_pos"], g["frames_vel"], g["frames_mass"], 3, keep_frames=True,
+                                  single=True)
+    assert np.array_equal(frames, g["frames"])
+
+
+def test_float_build_root_cube(orc, golden):
+    """FLOAT root cube: float(lo + hi) / 2 and float(extent + 2) (src/main.cpp:898-920)."""
+    g = golden("forces_float.npz")
+    c, s = orc.root_cube(g["split_pos"], single=True)
+    p32 = g["split_pos"].astype(np.float32)
+    lo, hi = p32.min(0), p32.max(0)
+    assert np.array_equal(c, ((lo + hi).astype(np.float64) / 2.0).astype(np.float32).astype(np.float64))
+    ext = hi - lo
+    assert s == float(np.float32(float(ext.max()) + 2.0))
+    c64, _ = orc.root_cube(g["split_pos"])
+    assert not np.array_equal(c, c64)
+
+
+@pytest.mark.parametrize("gt,n,theta,damp", [(0, 3000, 0.5, False), (1, 4000, 0.3, True), (2, 4000, 0.7, False)])
+def test_float_oracle_equals_float_reference_live(orc, oracle_mod, gt, n, theta, damp):
+    import os
+    if not os.path.exists(oracle_mod.REF_LIB_F32):
+        pytest.skip("FLOAT reference harness not built (oracle/_ref)")
+    R = oracle_mod.Reference(oracle_mod.REF_LIB_F32)
+    p, v, m = R.generate(oracle_mod.GenParams(gen_type=gt, size=1024 if gt else 512), n)
+    a_ref, _ = R.forces(p, m, theta, damping=damp)
+    a_or, _ = orc.forces(p, m, theta, damping=damp, single=True)
+    assert np.array_equal(a_ref, a_or)
+    t_ref = R.tree_nodes(p, m)
+    t_or = orc.tree_nodes(p, m, single=True)
+    for k in ("level", "count", "min_index", "mass", "com", "side"):
+        assert np.array_equal(t_ref[k], t_or[k]), k
