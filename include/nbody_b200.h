@@ -38,7 +38,8 @@
 extern "C" {
 #endif
 
-#define NBODY_ABI_VERSION 3  /* 2: nbody_params.autotune, nbody_stats walk fields; 3: merging */
+#define NBODY_ABI_VERSION 4  /* 2: nbody_params.autotune, nbody_stats walk fields; 3: merging;
+                                4: nbody_params.datatype_bytes */
 
 /* ---- status codes ---------------------------------------------------- */
 #define NBODY_OK 0
@@ -76,6 +77,16 @@ typedef struct nbody_params {
     double min_node_size;   /* key `min_node_size` (src/main.cpp:159): > 0 merges every cell
                                smaller than this into one particle before the forces
                                (apply_minimum_size, src/main.cpp:1001-1060) */
+    int datatype_bytes;     /* the reference build whose decisions to reproduce: 8 = DOUBLE
+                               (-DDOUBLE, default), 4 = FLOAT (-DFLOAT, the build its makefile
+                               ships, makefile:3). With 4, positions, velocities and masses are
+                               read as floats, and the root cube, child centres, node masses and
+                               centres of mass, the opening test side/distance > theta and the
+                               update are computed in float as that build computes them
+                               (src/vector.h:4-13, src/octree.cpp:54-85, 203-313,
+                               src/main.cpp:377, 887-927, src/particle.cpp:66-74), so accepted
+                               nodes equal the FLOAT build's. Pair forces follow `precision`.
+                               Merging and the adjoint need 8. */
 } nbody_params;
 
 /* Defaults of the reference's set_default (src/main.cpp:1312-1357) for the keys above;

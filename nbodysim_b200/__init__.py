@@ -49,6 +49,7 @@ class Params(C.Structure):
         ("min_adaptive_dt", C.c_double), ("max_pos_change", C.c_double), ("max_vel_change", C.c_double),
         ("precision", C.c_int), ("device", C.c_int), ("autotune", C.c_int),
         ("collide", C.c_int), ("collision_range", C.c_double), ("min_node_size", C.c_double),
+        ("datatype_bytes", C.c_int),
     ]
 
 

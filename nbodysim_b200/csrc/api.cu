@@ -133,6 +133,9 @@ struct nbody_ctx {
 
 namespace {
 
+// The reference's FLOAT build: decisions and node values follow its float arithmetic.
+bool single(const nbody_ctx *c) { return c->p.datatype_bytes == 4; }
+
 int set_device(nbody_ctx *c) {
     NB_CUDA(cudaSetDevice(c->p.device));
     return NBODY_OK;
@@ -150,6 +153,10 @@ int check_params(const nbody_params *p) {
         return fail(NBODY_ERR_INVALID, "collision_range must be finite and >= 0%s");
     if (!(p->min_node_size >= 0) || !std::isfinite(p->min_node_size))
         return fail(NBODY_ERR_INVALID, "min_node_size must be finite and >= 0%s");
+    if (p->datatype_bytes != 8 && p->datatype_bytes != 4)
+        return fail(NBODY_ERR_INVALID, "datatype_bytes must be 8 (DOUBLE build) or 4 (FLOAT build)%s");
+    if (p->datatype_bytes == 4 && (p->collide || p->min_node_size > 0))
+        return fail(NBODY_ERR_INVALID, "collisions and min_node_size need datatype_bytes 8%s");
     return NBODY_OK;
 }
 
@@ -257,6 +264,7 @@ void tree_inputs(nbody_ctx *c, uint32_t n, bool want_vmax) {
     tb.mass_ready = c->mass_pending;
     tb.vel_for_max = want_vmax ? c->vel : nullptr;
     tb.sc = c->sc;
+    tb.single = single(c) ? 1 : 0;
 }
 
 void ev(nbody_ctx *c, int k) {
@@ -313,6 +321,7 @@ int force_pass(nbody_ctx *c, int damping, double theta, bool fp64, bool want_vma
     a.t.sc = c->sc;
     a.theta = theta;
     a.damping = damping;
+    a.single = single(c) ? 1 : 0;
     a.accf = fp64 ? nullptr : (float *)c->acc;
     a.accd = fp64 ? (double *)c->acc : nullptr;
     a.counts = want_counts ? c->counts : nullptr;
@@ -602,7 +611,8 @@ int apply_collisions(nbody_ctx *c, unsigned *launches) {
 
 int one_step(nbody_ctx *c) {
     const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
-    StepParams sp{c->p.dt, c->p.adaptive, c->p.min_adaptive_dt, c->p.max_pos_change, c->p.max_vel_change};
+    StepParams sp{c->p.dt, c->p.adaptive, c->p.min_adaptive_dt, c->p.max_pos_change, c->p.max_vel_change,
+                  single(c)};
     const bool merge = merging(c);
     int rc = force_pass(c, c->p.damping, c->p.theta, fp64, c->p.adaptive != 0, c->p.adaptive != 0, false, false,
                         nullptr, false, nullptr, merge);
@@ -868,6 +878,7 @@ void nbody_default_params(nbody_params *p) {
     p->collide = 0;              // src/main.cpp:1353
     p->collision_range = 0.01;   // src/main.cpp:1354
     p->min_node_size = 0.0;      // src/main.cpp:1355
+    p->datatype_bytes = 8;       // the DOUBLE build (src/vector.h:4-13)
 }
 
 int nbody_create(const nbody_params *p, nbody_ctx **out) {
@@ -1170,7 +1181,8 @@ int nbody_step_host(nbody_ctx *c, uint32_t n, double *pos, double *vel, const do
             return rc;
         }
         const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
-        StepParams sp{c->p.dt, c->p.adaptive, c->p.min_adaptive_dt, c->p.max_pos_change, c->p.max_vel_change};
+        StepParams sp{c->p.dt, c->p.adaptive, c->p.min_adaptive_dt, c->p.max_pos_change, c->p.max_vel_change,
+                      single(c)};
         c->mass_pending = c->ev_mass;
         rc = force_pass(c, c->p.damping, c->p.theta, fp64, false, false, false, false);
         c->mass_pending = nullptr;
@@ -1250,6 +1262,7 @@ int nbody_force_vjp(nbody_ctx *c, uint32_t n, const double *pos, const double *m
     CTX_OR_FAIL(c);
     if (n > kMaxParticles) return fail(NBODY_ERR_INVALID, "n exceeds the 2^28 particle limit%s");
     if (n && (!pos || !mass || !dL_dacc || !dL_dpos || !dL_dmass)) return fail(NBODY_ERR_INVALID, "null array%s");
+    if (single(c)) return fail(NBODY_ERR_INVALID, "the adjoint needs datatype_bytes 8%s");
     if (n == 0) return NBODY_OK;
     int rc = upload(c, n, pos, nullptr, mass);
     if (rc) return rc;
@@ -1278,6 +1291,7 @@ int nbody_forward_checkpointed(nbody_ctx *c, uint32_t nsteps, uint32_t every) {
     if (!c->have_state || !c->have_vel) return fail(NBODY_ERR_STATE, "particles with velocities must be set first%s");
     if (c->p.adaptive) return fail(NBODY_ERR_INVALID, "the adjoint needs a fixed dt (adaptive = 0)%s");
     if (merging(c)) return fail(NBODY_ERR_INVALID, "the adjoint cannot differentiate through merging%s");
+    if (single(c)) return fail(NBODY_ERR_INVALID, "the adjoint needs datatype_bytes 8%s");
     c->have_fwd = false;
     if (nsteps == 0 || c->n == 0) return NBODY_OK;
     if (every == 0) {

@@ -11,6 +11,8 @@ namespace nbody {
 //   dt_k = clamp(min(dt, max_vel_change / max|a|, max_pos_change / max|v|),
 //                min_adaptive_dt, dt)
 // with clamp as src/main.cpp:177-182 defines it and |v| taken before the kick.
+// The FLOAT build (single) does the same in float: the state and dt are read
+// as floats and every product and sum is rounded to float.
 template <typename AccT>
 __global__ void k_update(double *__restrict__ pos, double *__restrict__ vel, const AccT *__restrict__ acc,
                          uint32_t n, StepParams sp, DevScalars *sc) {
@@ -28,6 +30,17 @@ __global__ void k_update(double *__restrict__ pos, double *__restrict__ vel, con
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) sc->dt_used = dt;
     if (i >= n) return;
+    if (sp.single) {
+        const float fdt = __double2float_rn(dt);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const size_t o = 3 * (size_t)i + k;
+            const float v = __fadd_rn(__double2float_rn(vel[o]), __fmul_rn(__double2float_rn((double)acc[o]), fdt));
+            vel[o] = (double)v;
+            pos[o] = (double)__fadd_rn(__double2float_rn(pos[o]), __fmul_rn(v, fdt));
+        }
+        return;
+    }
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         const size_t o = 3 * (size_t)i + k;

@@ -11,6 +11,7 @@ struct StepParams {
     double dt;
     int adaptive;
     double min_adaptive_dt, max_pos_change, max_vel_change;
+    int single;  // the reference's FLOAT build: the update in float arithmetic
 };
 
 cudaError_t launch_update(double *pos, double *vel, const void *acc, bool acc_double, uint32_t n,

@@ -15,12 +15,40 @@
 namespace nbody {
 
 // ---------------------------------------------------------------------------
-// Root cube: bbox midpoint; side = largest extent + 2.0, a tie for the largest
-// extent falls through to the z extent (src/main.cpp:898-920). Also flags
+// Root cube from the extrema: bbox midpoint; side = largest extent + 2.0, a tie
+// for the largest extent falls through to the z extent (src/main.cpp:898-920).
+// The FLOAT build computes it from float extrema (the extrema of the rounded
+// positions are the rounded extrema): center = float(lo + hi) / 2.0 rounded to
+// float, extents in float, side = float(extent + 2.0).
+__device__ inline void root_from_extrema(const double *lo, const double *hi, bool single, double *center,
+                                         double *side) {
+    if (single) {
+        float l[3], h[3];
+        for (int k = 0; k < 3; k++) {
+            l[k] = __double2float_rn(lo[k]);
+            h[k] = __double2float_rn(hi[k]);
+            center[k] = (double)__double2float_rn(__dmul_rn((double)__fadd_rn(l[k], h[k]), 0.5));
+        }
+        const float ex = __fsub_rn(h[0], l[0]), ey = __fsub_rn(h[1], l[1]), ez = __fsub_rn(h[2], l[2]);
+        float e;
+        if (ex > ey && ex > ez) e = ex;
+        else if (ey > ex && ey > ez) e = ey;
+        else e = ez;
+        *side = (double)__double2float_rn(__dadd_rn((double)e, 2.0));
+        return;
+    }
+    for (int k = 0; k < 3; k++) center[k] = (lo[k] + hi[k]) / 2.0;
+    const double ex = hi[0] - lo[0], ey = hi[1] - lo[1], ez = hi[2] - lo[2];
+    if (ex > ey && ex > ez) *side = ex + 2.0;
+    else if (ey > ex && ey > ez) *side = ey + 2.0;
+    else *side = ez + 2.0;
+}
+
+// Root cube (root_from_extrema) over all particles. Also flags
 // non-finite positions (masses are checked where the bodies are gathered), and
 // (optionally) reduces max |v| for the adaptive step.
 __global__ void k_bbox(const double *__restrict__ pos, const double *__restrict__ vel, uint32_t n,
-                       double *__restrict__ partial, DevScalars *sc, int keep_root) {
+                       double *__restrict__ partial, DevScalars *sc, int keep_root, int single) {
     __shared__ double s_red[7][32];
     __shared__ bool s_last;
     double mn[3] = {INFINITY, INFINITY, INFINITY};
@@ -74,13 +102,10 @@ __global__ void k_bbox(const double *__restrict__ pos, const double *__restrict_
         for (int k = 0; k < 3; k++) {
             sc->bbox_min[k] = lo[k];
             sc->bbox_max[k] = hi[k];
-            sc->root_center[k] = (lo[k] + hi[k]) / 2.0;
         }
-        double ex = hi[0] - lo[0], ey = hi[1] - lo[1], ez = hi[2] - lo[2];
-        double side;
-        if (ex > ey && ex > ez) side = ex + 2.0;
-        else if (ey > ex && ey > ez) side = ey + 2.0;
-        else side = ez + 2.0;
+        double center[3], side;
+        root_from_extrema(lo, hi, single != 0, center, &side);
+        for (int k = 0; k < 3; k++) sc->root_center[k] = center[k];
         sc->root_side = side;
         sc->max_vel_bits = (unsigned long long)__double_as_longlong(-r[6]);
         sc->ticket = 0;
@@ -90,7 +115,7 @@ __global__ void k_bbox(const double *__restrict__ pos, const double *__restrict_
 // Root cube per system (several independent systems): one block per system.
 __global__ void k_bbox_systems(const double *__restrict__ pos, const double *__restrict__ mass,
                                const uint32_t *__restrict__ sys_start, double *__restrict__ sys_root,
-                               DevScalars *sc) {
+                               DevScalars *sc, int single) {
     __shared__ double s_red[6][32];
     const uint32_t b0 = sys_start[blockIdx.x], b1 = sys_start[blockIdx.x + 1];
     double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -116,13 +141,7 @@ __global__ void k_bbox_systems(const double *__restrict__ pos, const double *__r
     if (lane == 0) {
         const double lo[3] = {r[0], r[1], r[2]}, hi[3] = {-r[3], -r[4], -r[5]};
         double *o = sys_root + 4 * (size_t)blockIdx.x;
-        for (int k = 0; k < 3; k++) o[k] = (lo[k] + hi[k]) / 2.0;
-        const double ex = hi[0] - lo[0], ey = hi[1] - lo[1], ez = hi[2] - lo[2];
-        double side;
-        if (ex > ey && ex > ez) side = ex + 2.0;
-        else if (ey > ex && ey > ez) side = ey + 2.0;
-        else side = ez + 2.0;
-        o[3] = side;
+        root_from_extrema(lo, hi, single != 0, o, o + 3);
     }
 }
 
@@ -131,22 +150,34 @@ __global__ void k_bbox_systems(const double *__restrict__ pos, const double *__r
 // exactly as allocate_child does (src/octree.cpp:65-84: center + (+-1 * half) / 2
 // with half = side / 2), and choosing the octant with strict '>' as
 // add_particle does (src/octree.cpp:153-165). Digits are (z<<2)|(y<<1)|x so
-// that Morton order equals the reference's child order 0..7.
-__device__ inline uint64_t descend_word(double x, double y, double z, double &cx, double &cy,
-                                        double &cz, double &side) {
+// that Morton order equals the reference's child order 0..7. T is the
+// reference build's datatype: double, or float for its FLOAT build.
+__device__ inline double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ inline float add_rn(float a, float b) { return __fadd_rn(a, b); }
+
+template <typename T>
+__device__ inline uint64_t descend_word(T x, T y, T z, T &cx, T &cy, T &cz, T &side) {
     uint64_t key = 0;
 #pragma unroll 3
     for (int l = 0; l < kLevelsPerWord; l++) {
-        double half = side / 2;
-        double q = half / 2;
+        const T half = side / T(2);
+        const T q = half / T(2);
         int bx = x > cx, by = y > cy, bz = z > cz;
         key = (key << 3) | (uint64_t)((bz << 2) | (by << 1) | bx);
-        cx = __dadd_rn(cx, bx ? q : -q);
-        cy = __dadd_rn(cy, by ? q : -q);
-        cz = __dadd_rn(cz, bz ? q : -q);
+        cx = add_rn(cx, bx ? q : -q);
+        cy = add_rn(cy, by ? q : -q);
+        cz = add_rn(cz, bz ? q : -q);
         side = half;
     }
     return key;
+}
+
+// `words` key words of one particle from the root cube (center, side).
+template <typename T>
+__device__ inline void descend_words(const double *p, const double *root, int words, uint64_t *out) {
+    T cx = (T)root[0], cy = (T)root[1], cz = (T)root[2], s = (T)root[3];
+    const T x = (T)p[0], y = (T)p[1], z = (T)p[2];
+    for (int w = 0; w < words; w++) out[w] = descend_word<T>(x, y, z, cx, cy, cz, s);
 }
 
 // Two key words per particle: levels 1..21 (k1) and 22..42 (k2). Escaped
@@ -155,23 +186,24 @@ __device__ inline uint64_t descend_word(double x, double y, double z, double &cx
 __global__ void k_keys(const double *__restrict__ pos, uint32_t n, const DevScalars *sc,
                        uint64_t *__restrict__ k1_user, uint64_t *__restrict__ k2_sortkey,
                        uint64_t *__restrict__ k2_user, uint32_t *__restrict__ idx,
-                       const uint32_t *__restrict__ sys_id, const double *__restrict__ sys_root) {
+                       const uint32_t *__restrict__ sys_id, const double *__restrict__ sys_root, int single) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    double cx, cy, cz, side;
+    double root[4];
     if (sys_id) {
         const double *r = sys_root + 4 * (size_t)sys_id[i];
-        cx = r[0]; cy = r[1]; cz = r[2]; side = r[3];
+        root[0] = r[0]; root[1] = r[1]; root[2] = r[2]; root[3] = r[3];
     } else {
-        cx = sc->root_center[0]; cy = sc->root_center[1]; cz = sc->root_center[2];
-        side = sc->root_side;
+        root[0] = sc->root_center[0]; root[1] = sc->root_center[1]; root[2] = sc->root_center[2];
+        root[3] = sc->root_side;
     }
-    const double x = pos[3 * (size_t)i], y = pos[3 * (size_t)i + 1], z = pos[3 * (size_t)i + 2];
-    const uint64_t a = descend_word(x, y, z, cx, cy, cz, side);
-    const uint64_t b = descend_word(x, y, z, cx, cy, cz, side);
-    k1_user[i] = a;
-    k2_sortkey[i] = b;
-    k2_user[i] = b;
+    const double p[3] = {pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2]};
+    uint64_t w[2];
+    if (single) descend_words<float>(p, root, 2, w);
+    else descend_words<double>(p, root, 2, w);
+    k1_user[i] = w[0];
+    k2_sortkey[i] = w[1];
+    k2_user[i] = w[1];
     idx[i] = i;
 }
 
@@ -267,16 +299,21 @@ unsigned scan_exclusive(uint32_t *v, uint32_t len, uint32_t *tile_sums, uint32_t
 }
 
 // ---------------------------------------------------------------------------
-// Bodies in sorted order; flags non-finite masses.
+// Bodies in sorted order (as floats in the FLOAT build); flags non-finite masses.
 __global__ void k_gather_bodies(const uint32_t *__restrict__ idx, const double *__restrict__ pos,
                                 const double *__restrict__ mass, double4 *__restrict__ body,
-                                uint32_t n, DevScalars *sc) {
+                                uint32_t n, DevScalars *sc, int single) {
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     uint32_t i = idx[j];
-    const double m = mass[i];
+    double m = mass[i];
     if (!isfinite(m)) atomicOr(&sc->status, kStatusNonFinite);
-    body[j] = make_double4(pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2], m);
+    double4 b = make_double4(pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2], m);
+    if (single) {
+        b.x = (double)__double2float_rn(b.x); b.y = (double)__double2float_rn(b.y);
+        b.z = (double)__double2float_rn(b.z); b.w = (double)__double2float_rn(b.w);
+    }
+    body[j] = b;
 }
 
 // Groups of particles whose 42-level keys agree get a third key word (levels
@@ -287,7 +324,7 @@ constexpr int kMaxDeepGroup = 64;
 __global__ void k_deep_groups(const uint64_t *__restrict__ key1, const uint64_t *__restrict__ key2,
                               uint64_t *__restrict__ key3, uint32_t *__restrict__ idx,
                               double4 *__restrict__ body, uint32_t n, const uint32_t *__restrict__ sys,
-                              const double *__restrict__ sys_root, DevScalars *sc) {
+                              const double *__restrict__ sys_root, DevScalars *sc, int single) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i + 1 >= n) return;
     const uint64_t k = key1[i], kk = key2[i];
@@ -308,18 +345,18 @@ __global__ void k_deep_groups(const uint64_t *__restrict__ key1, const uint64_t 
         atomicOr(&sc->status, kStatusCoincident);
         return;
     }
-    double rcx = sc->root_center[0], rcy = sc->root_center[1], rcz = sc->root_center[2];
-    double rs = sc->root_side;
+    double root[4] = {sc->root_center[0], sc->root_center[1], sc->root_center[2], sc->root_side};
     if (sys) {
         const double *r = sys_root + 4 * (size_t)ss;
-        rcx = r[0]; rcy = r[1]; rcz = r[2]; rs = r[3];
+        root[0] = r[0]; root[1] = r[1]; root[2] = r[2]; root[3] = r[3];
     }
     for (uint32_t j = i; j <= e; j++) {
         const double4 b = body[j];
-        double cx = rcx, cy = rcy, cz = rcz, s = rs;
-        descend_word(b.x, b.y, b.z, cx, cy, cz, s);
-        descend_word(b.x, b.y, b.z, cx, cy, cz, s);
-        key3[j] = descend_word(b.x, b.y, b.z, cx, cy, cz, s);
+        const double p[3] = {b.x, b.y, b.z};
+        uint64_t w[3];
+        if (single) descend_words<float>(p, root, 3, w);
+        else descend_words<double>(p, root, 3, w);
+        key3[j] = w[2];
     }
     // insertion sort of the group by its third word
     for (uint32_t j = i + 1; j <= e; j++) {
@@ -485,6 +522,59 @@ __device__ inline double3 load_node_com(const double4 *p, double &m) {
     return make_double3(a.x, a.y, b.x);
 }
 
+// Round-to-nearest arithmetic of the reference build's datatype.
+__device__ inline double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ inline float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ inline double div_rn(double a, double b) { return __ddiv_rn(a, b); }
+__device__ inline float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+
+// One node's mass and centre of mass from its children, in the arithmetic of
+// T (double, or float for the reference's FLOAT build).
+template <typename T>
+__device__ inline double4 node_com(const double4 *__restrict__ body, const int32_t *__restrict__ ochild,
+                                   const int32_t *__restrict__ ometa, const double4 *onode, int p, int L, int nch) {
+    T m = 0, sx = 0, sy = 0, sz = 0;
+    for (int k = 0; k < nch; k++) {
+        const int c = ochild[8 * p + k];
+        T cmk, cx, cy, cz;
+        if (c < 0) {
+            const double4 b = body[~c];
+            cmk = (T)b.w;
+            cx = (T)b.x; cy = (T)b.y; cz = (T)b.z;
+        } else {
+            double dm;
+            const double3 cc = load_node_com(&onode[c], dm);
+            cmk = (T)dm;
+            cx = (T)cc.x; cy = (T)cc.y; cz = (T)cc.z;
+            const int chain = meta_level(ometa[c]) - L - 1;
+            for (int t = 0; t < chain; t++) {
+                if (cmk == T(0)) {
+                    cx = cy = cz = T(0);
+                } else {
+                    cx = div_rn(mul_rn(cx, cmk), cmk);
+                    cy = div_rn(mul_rn(cy, cmk), cmk);
+                    cz = div_rn(mul_rn(cz, cmk), cmk);
+                }
+            }
+        }
+        m = add_rn(m, cmk);
+        sx = add_rn(sx, mul_rn(cx, cmk));
+        sy = add_rn(sy, mul_rn(cy, cmk));
+        sz = add_rn(sz, mul_rn(cz, cmk));
+    }
+    double4 out;
+    out.w = (double)m;
+    if (m == T(0)) {
+        out.x = out.y = out.z = 0.0;
+    } else {
+        out.x = (double)div_rn(sx, m);
+        out.y = (double)div_rn(sy, m);
+        out.z = (double)div_rn(sz, m);
+    }
+    return out;
+}
+
+template <typename T>
 __global__ void k_com(const double4 *__restrict__ body, const int32_t *__restrict__ leaf_oparent,
                       const int32_t *__restrict__ oparent, const int32_t *__restrict__ ochild,
                       const int32_t *__restrict__ ometa, double4 *onode, uint32_t *ocount,
@@ -515,42 +605,7 @@ __global__ void k_com(const double4 *__restrict__ body, const int32_t *__restric
         // The reference sums the masses, then the mass-weighted centres, each in
         // child order; both sums run here in one pass over the children.
         const int L = meta_level(meta);
-        double m = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
-        for (int k = 0; k < nch; k++) {
-            const int c = ochild[8 * p + k];
-            double cmk;
-            double3 cck;
-            if (c < 0) {
-                const double4 b = body[~c];
-                cmk = b.w;
-                cck = make_double3(b.x, b.y, b.z);
-            } else {
-                cck = load_node_com(&onode[c], cmk);
-                const int chain = meta_level(ometa[c]) - L - 1;
-                for (int t = 0; t < chain; t++) {
-                    if (cmk == 0.0) {
-                        cck = make_double3(0.0, 0.0, 0.0);
-                    } else {
-                        cck.x = __ddiv_rn(__dmul_rn(cck.x, cmk), cmk);
-                        cck.y = __ddiv_rn(__dmul_rn(cck.y, cmk), cmk);
-                        cck.z = __ddiv_rn(__dmul_rn(cck.z, cmk), cmk);
-                    }
-                }
-            }
-            m = __dadd_rn(m, cmk);
-            sx = __dadd_rn(sx, __dmul_rn(cck.x, cmk));
-            sy = __dadd_rn(sy, __dmul_rn(cck.y, cmk));
-            sz = __dadd_rn(sz, __dmul_rn(cck.z, cmk));
-        }
-        double4 out;
-        out.w = m;
-        if (m == 0.0) {
-            out.x = out.y = out.z = 0.0;
-        } else {
-            out.x = __ddiv_rn(sx, m);
-            out.y = __ddiv_rn(sy, m);
-            out.z = __ddiv_rn(sz, m);
-        }
+        const double4 out = node_com<T>(body, ochild, ometa, onode, p, L, nch);
         double2 *q = reinterpret_cast<double2 *>(&onode[p]);
         __stcg(q, make_double2(out.x, out.y));
         __stcg(q + 1, make_double2(out.z, out.w));
@@ -568,15 +623,15 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
     const bool multi = tb.nsys > 1;
     // root cube (+ max |v| when requested); one per system when there are several
     k_bbox<<<tb.bbox_blocks, 256, 0, st>>>(tb.pos, tb.vel_for_max, n, tb.bbox_partial, tb.sc,
-                                           multi ? 0 : tb.keep_root);
+                                           multi ? 0 : tb.keep_root, tb.single);
     if (multi) {
         if (tb.mass_ready) cudaStreamWaitEvent(st, tb.mass_ready, 0);
-        k_bbox_systems<<<tb.nsys, 256, 0, st>>>(tb.pos, tb.mass, tb.sys_start, tb.sys_root, tb.sc);
+        k_bbox_systems<<<tb.nsys, 256, 0, st>>>(tb.pos, tb.mass, tb.sys_start, tb.sys_root, tb.sc, tb.single);
         L += 1;
     }
     // keys: k1 (user order) -> key3, k2 -> key_a (sort key) and key2 (user order)
     k_keys<<<blocks_for(n, 256), 256, 0, st>>>(tb.pos, n, tb.sc, tb.key3, tb.key_a, tb.key2, tb.idx_a,
-                                               multi ? tb.sys_id : nullptr, tb.sys_root);
+                                               multi ? tb.sys_id : nullptr, tb.sys_root, tb.single);
     L += 2;
     // LSD radix sort by (system, k1, k2): 8 passes on k2, 8 on k1, 2 on the system id.
     cudaError_t e = sort_prepare(tb.key2, tb.key3, multi ? tb.sys_id : nullptr, n, multi ? 18 : 16, tb.sort_scratch,
@@ -603,14 +658,14 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
     }
     k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key2, tb.idx_a, tb.key_a, n);  // k2 sorted
     if (tb.mass_ready && !multi) cudaStreamWaitEvent(st, tb.mass_ready, 0);  // the first reader of the masses
-    k_gather_bodies<<<blocks_for(n, 256), 256, 0, st>>>(tb.idx_a, tb.pos, tb.mass, tb.body, n, tb.sc);
+    k_gather_bodies<<<blocks_for(n, 256), 256, 0, st>>>(tb.idx_a, tb.pos, tb.mass, tb.body, n, tb.sc, tb.single);
     L += 3;
     *launches += L;
     if (n < 2) return cudaGetLastError();
     L = 0;
     const uint32_t *sys_sorted = multi ? tb.sys_sorted : nullptr;
     k_deep_groups<<<blocks_for(n, 256), 256, 0, st>>>(tb.key_b, tb.key_a, tb.key3, tb.idx_a, tb.body, n,
-                                                       sys_sorted, tb.sys_root, tb.sc);
+                                                       sys_sorted, tb.sys_root, tb.sc, tb.single);
     KeyView kv{tb.key_b, tb.key_a, tb.key3, (int)n, sys_sorted};
     const uint32_t m = n - 1;
     k_radix_tree<<<blocks_for(m, 256), 256, 0, st>>>(kv, tb.bleft, tb.bright, tb.bparent, tb.leaf_bparent,
@@ -640,8 +695,12 @@ cudaError_t compute_com(const TreeBuild &tb, cudaStream_t st, unsigned *launches
     if (n < 2) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(tb.ocount, 0, sizeof(uint32_t) * (n - 1), st);
     if (e != cudaSuccess) return e;
-    k_com<<<blocks_for(n - 1, 256), 256, 0, st>>>(tb.body, tb.leaf_oparent, tb.oparent, tb.ochild, tb.ometa,
-                                              tb.onode, tb.ocount, n, tb.sc);
+    if (tb.single)
+        k_com<float><<<blocks_for(n - 1, 256), 256, 0, st>>>(tb.body, tb.leaf_oparent, tb.oparent, tb.ochild,
+                                                             tb.ometa, tb.onode, tb.ocount, n, tb.sc);
+    else
+        k_com<double><<<blocks_for(n - 1, 256), 256, 0, st>>>(tb.body, tb.leaf_oparent, tb.oparent, tb.ochild,
+                                                              tb.ometa, tb.onode, tb.ocount, n, tb.sc);
     *launches += 1;
     return cudaGetLastError();
 }

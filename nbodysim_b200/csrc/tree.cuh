@@ -13,6 +13,9 @@ struct TreeBuild {
                                 // the build waits for this event before it first reads them
     const double *vel_for_max;  // non-null: also reduce max |v| (adaptive dt)
     int keep_root;              // rebuild inside the root cube already in sc (single system)
+    int single;                 // the reference's FLOAT build: positions and masses are read as
+                                // floats; root cube, child centres, node masses and centres of
+                                // mass are computed in float arithmetic
     DevScalars *sc;
     double *bbox_partial;       // 7 * bbox_blocks
     unsigned bbox_blocks;

@@ -97,6 +97,27 @@ __device__ inline bool exact_open(double cx, double cy, double cz, double px, do
     return __ddiv_rn(side, d) > theta;
 }
 
+// The same test as the reference's FLOAT build evaluates it: float
+// differences, their squares summed in double (pow(float, 2) promotes), the
+// double square root rounded to float, then float side / float distance
+// against float theta (src/main.cpp:377, src/vector.cpp:99-102, datatype float).
+__device__ inline bool exact_open_f32(double cx, double cy, double cz, double px, double py, double pz,
+                                      double side, float theta) {
+    const float dx = __fsub_rn((float)cx, (float)px), dy = __fsub_rn((float)cy, (float)py),
+                dz = __fsub_rn((float)cz, (float)pz);
+    const double s = __dadd_rn(__dadd_rn(__dmul_rn((double)dx, (double)dx), __dmul_rn((double)dy, (double)dy)),
+                               __dmul_rn((double)dz, (double)dz));
+    const float d = __double2float_rn(__dsqrt_rn(s));
+    return __fdiv_rn(__double2float_rn(side), d) > theta;
+}
+
+// The reference's opening test in the build's datatype.
+__device__ inline bool ref_open(bool single, double cx, double cy, double cz, double px, double py, double pz,
+                                double side, double theta, float theta_f) {
+    return single ? exact_open_f32(cx, cy, cz, px, py, pz, side, theta_f)
+                  : exact_open(cx, cy, cz, px, py, pz, side, theta);
+}
+
 // Moves the oldest half of a full stack to this warp's global spill region.
 template <class Sm>
 __device__ inline bool spill_out(Sm &s, int &top, uint32_t &spill_top, int2 *gspill, uint32_t spill_cap,
@@ -417,7 +438,12 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
     Sm &s = reinterpret_cast<Sm *>(smem_raw)[wid];
     const Tree &t = a.t;
     const uint32_t n = t.n;
-    const double theta = a.theta;
+    const bool single = a.single != 0;
+    const float theta_f = __double2float_rn(a.theta);
+    const double theta = single ? (double)theta_f : a.theta;
+    // relative width of the FP64 form's group-level band: its own rounding, or
+    // the FLOAT build's (~6.3 float ulps of (side/theta)^2)
+    const double grp_rel = single ? 1e-6 : 1e-12;
     const double S1 = t.sc->root_side;
     int2 *gspill = a.spill + (size_t)(blockIdx.x * (blockDim.x >> 5) + wid) * a.spill_cap;
     const unsigned FULL = 0xffffffffu;
@@ -566,7 +592,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                                  bz_ = fmax(fabs(oz - dloz), fabs(oz - dhiz));
                     const double r2min = ax_ * ax_ + ay_ * ay_ + az_ * az_;
                     const double r2max = bx_ * bx_ + by_ * by_ + bz_ * bz_;
-                    const double tol = 1e-12 * (qd + dpm * sq) + 1e-300;
+                    const double tol = grp_rel * (qd + dpm * sq) + 1e-300;
                     if (r2min - qd > tol) my_open = 0;
                     else if (qd - r2max > tol) my_open = reach;
                     else mixed = true;
@@ -609,10 +635,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                         mm &= mm - 1;
                         const double4 c = s.tc[k];
                         const uint32_t rk = (uint32_t)s.tr[k].x;
-                        const double dx = __dsub_rn(c.x, b.x), dy = __dsub_rn(c.y, b.y), dz = __dsub_rn(c.z, b.z);
-                        const double d = __dsqrt_rn(
-                            __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
-                        const bool open = __ddiv_rn(c.w, d) > theta;
+                        const bool open = ref_open(single, c.x, c.y, c.z, b.x, b.y, b.z, c.w, theta, theta_f);
                         const uint32_t om = __ballot_sync(FULL, open) & rk;
                         if (lane == k) my_open = om;
                     }
@@ -640,14 +663,14 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                                 const int node = __float_as_int(q1.w);
                                 const double4 nd = t.onode[node];
                                 const double side = s.gc.S * exp2_neg(meta_level(t.ometa[node]));
-                                open1 = exact_open(nd.x, nd.y, nd.z, b.x, b.y, b.z, side, theta);
+                                open1 = ref_open(single, nd.x, nd.y, nd.z, b.x, b.y, b.z, side, theta, theta_f);
                                 nfallback++;
                             }
                             if (amb2) {
                                 const int node = __float_as_int(q2.w);
                                 const double4 nd = t.onode[node];
                                 const double side = s.gc.S * exp2_neg(meta_level(t.ometa[node]));
-                                open2 = exact_open(nd.x, nd.y, nd.z, b.x, b.y, b.z, side, theta);
+                                open2 = ref_open(single, nd.x, nd.y, nd.z, b.x, b.y, b.z, side, theta, theta_f);
                                 nfallback++;
                             }
                         }

@@ -16,6 +16,9 @@ struct WalkArgs {
     Tree t;
     double theta;
     int damping;
+    // The reference's FLOAT build: node values are floats and the opening test
+    // is its float expression (float theta, float side / float distance).
+    int single;
     float *accf;        // MIXED: user order, 3 floats per particle
     double *accd;       // FP64: user order, 3 doubles per particle
     uint32_t *counts;   // optional: accepted nodes per particle (user order)

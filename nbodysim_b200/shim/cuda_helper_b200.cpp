@@ -17,9 +17,11 @@
 //
 // Build: compile this file with the reference's headers on the include path
 // and the same -DFLOAT / -DDOUBLE as the rest of the program, and link
-// libnbody_b200.so. In a FLOAT build the positions and
-// masses are widened to double for the library and the accelerations narrowed
-// back to float.
+// libnbody_b200.so. In a FLOAT build the positions and masses are widened to
+// double for the library (exactly), the library is told the program's
+// datatype (nbody_params.datatype_bytes = sizeof(datatype)) so that it builds
+// the tree and takes every opening decision in float as this build does, and
+// the accelerations are narrowed back to float.
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -45,6 +47,7 @@ Engine &engine() {
         nbody_default_params(&p);
         const char *prec = std::getenv("NBODY_B200_PRECISION");
         if (prec && prec[0] == 'f') p.precision = NBODY_PRECISION_FP64;
+        p.datatype_bytes = (int)sizeof(datatype);
         int rc = nbody_create(&p, &e.ctx);
         if (rc != NBODY_OK) {
             std::fprintf(stderr, "nbody_b200: %s: %s\n", nbody_status_string(rc), nbody_last_error_message());
