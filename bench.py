@@ -5,20 +5,24 @@ sphere of radius 100, masses uniform in [5e10, 5e11], rotation 0.1 about z,
 size 1024, theta 0.5, adaptive dt (min_adaptive_dt 0.00333, max_pos_change 3,
 max_vel_change 3). A step is one full pass of the hot path on the GPU: root
 cube -> Morton keys -> radix sort -> octree -> mass/COM -> fused walk + gravity
--> adaptive dt -> update.
+-> adaptive dt -> update. Every timed step starts from the seeded initial
+shell: the state is restored (and L2 flushed) outside the event pair, so both
+this arm and the reference arm walk the same particle state.
 
-  value        interactions/s over K resident steps (inputs already in HBM),
-               CUDA events on the engine's stream, max over ranks
-  e2e          the same metric through the C ABI with host buffers: every step
-               uploads pos/vel/mass from pinned memory and downloads pos/vel;
-               the same K steps from the same state as `value`
+  value        interactions/s over K steps with inputs resident in HBM, CUDA
+               events on the engine's stream around each step, max over ranks
+  e2e          the same K steps through the C ABI with host buffers: every step
+               uploads pos/vel/mass from pinned memory and downloads pos/vel
+  evolved      secondary: K consecutive steps of the collapsing shell after W
+               warm-up steps (interactions per step grow as it collapses)
   roofline     the fused walk kernel: 20 FLOP per interaction (the customary
                N-body count) against the measured FP32 FMA peak
-  cpu_baseline the reference's own CPU walk (oracle/_ref, all host threads, and
-               one thread under `single_thread`) on a bounded sample of the
-               same workload; also the reference's frame
-               loop on config 1, which checks the GPU's final positions
+  cpu_baseline the reference's own CPU path (oracle/_ref, release flags, all
+               host threads; one thread under `single_thread`) on a bounded
+               sample of the same initial state
 
+rank 0 prints one line of details (configs, adjoint with finite differences,
+ensemble) prefixed with "bench-details: ", then the JSON headline line.
 `--impl reference` times the reference's CPU implementation alone (rank 0).
 """
 from __future__ import annotations
@@ -40,6 +44,7 @@ UNIT = "interactions/s"
 FLOP_PER_INTERACTION = 20
 WORKLOAD = dict(gen_type=2, n=1 << 20, r_sphere=100.0, rotation_magnitude=0.1, size=1024.0,
                 min_mass=5e10, max_mass=5e11, seed=0xDEADBEEF)
+L2_FLUSH_BYTES = 256 << 20  # written between timed steps: twice the 126 MB L2
 
 
 def parse():
@@ -55,8 +60,8 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-configs", action="store_true", help="skip the cube / sphere / theta-sweep legs")
-    ap.add_argument("--adjoint-fd", type=int, default=0,
-                    help="also check the config-4 gradient against central differences on this many coordinates")
+    ap.add_argument("--adjoint-fd", type=int, default=64,
+                    help="check the adjoint against FP64 central differences on this many seeded coordinates")
     return ap.parse_args()
 
 
@@ -64,8 +69,9 @@ def workload_config(args) -> dict:
     return {"workload": f"shell N={args.n} theta={args.theta} adaptive dt", "gen_type": "shell",
             "n": args.n, "theta": args.theta, "r_sphere": 100.0, "size": 1024.0, "rotation_magnitude": 0.1,
             "adaptive_dt": {"min_adaptive_dt": 0.00333, "max_pos_change": 3.0, "max_vel_change": 3.0},
+            "state": "every timed step starts from the seeded initial shell, restored outside the event pair",
             "parallelism": f"replicas x{args.gpus}",
-            "l2": "working set (~300 MB per 1M particles) exceeds the 126 MB L2; no flush between steps"}
+            "l2": "flushed between timed steps (256 MB written); the step's working set (~300 MB) exceeds L2 too"}
 
 
 def dist_env():
@@ -136,14 +142,16 @@ def cpu_cores() -> int:
 
 
 def cpu_reference_sample(pos, mass, theta, seconds, threads, counts=None):
-    """The reference's own CPU path (oracle/_ref) on a bounded sample: tree +
-    mass/COM over all N, the walk for a seeded sample of particles. Returns
-    (interactions/s, description, kind, per-step seconds)."""
+    """The reference's own CPU path (oracle/_ref, the DOUBLE build with its release
+    flags where the host supports them) on a bounded sample: tree + mass/COM over
+    all N, the walk for a seeded sample of particles. Returns (interactions/s,
+    description, kind, per-step seconds)."""
     import oracle
     n = len(mass)
     kind = "reference"
+    lib = oracle.REF_LIB_REL if oracle.release_build_usable() else oracle.REF_LIB
     try:
-        R = oracle.Reference()
+        R = oracle.Reference(lib)
     except FileNotFoundError:
         R = None
         kind = "port"
@@ -172,7 +180,8 @@ def cpu_reference_sample(pos, mass, theta, seconds, threads, counts=None):
         orc.forces(pos, mass, theta, threads=threads, sample=sample)
         build, com, walk = 0.0, 0.0, time.perf_counter() - t0
     step_s = walk + (build + com) * m / n
-    desc = (f"{m} of {n} particles walked ({'reference barnes_hut_threaded' if R else 'oracle port'}, "
+    flags = "release flags -O2 -march=x86-64-v3" if lib == oracle.REF_LIB_REL else "-O2"
+    desc = (f"initial state: {m} of {n} particles walked ({'reference barnes_hut_threaded, ' + flags if R else 'oracle port'}, "
             f"{threads} threads); tree build {build:.3f}s + mass/COM {com:.3f}s over all N amortised by {m}/{n}; "
             f"walk {walk:.3f}s")
     return inter / step_s, desc, kind, step_s
@@ -187,10 +196,12 @@ def run_reference(args) -> None:
     g = oracle.GenParams(gen_type=2, size=1024.0, r_sphere=100.0, rotation_magnitude=0.1)
     pos, vel, mass = orc.generate(g, args.n)
     threads = cpu_cores()
+    # accepted nodes of every particle on this state (the reference's counts,
+    # through the oracle): the per-step interaction total the GPU arm also reports
+    _, counts = orc.forces(pos, mass, args.theta, threads=threads)
     seconds = max(1.0, min(args.cpu_seconds, 120.0 / max(1, args.steps + args.warmup)))
     vals = []
     desc, kind = "", "reference"
-    counts = None
     for s in range(args.warmup + args.steps):
         v, desc, kind, _ = cpu_reference_sample(pos, mass, args.theta, seconds, threads, counts)
         if s >= args.warmup:
@@ -200,6 +211,7 @@ def run_reference(args) -> None:
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded reference generator)",
             "config": workload_config(args),
+            "interactions_per_step": int(counts.sum(dtype=np.int64)),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -223,70 +235,103 @@ def run_ours(args) -> None:
     stream = torch.cuda.current_stream()
     g = nb.gen_params(gen_type=2, size=1024.0, r_sphere=100.0, rotation_magnitude=0.1, seed=0xDEADBEEF + rank)
     pos0, vel0, mass = nb.generate(args.n, g)
-    params = nb.default_params(theta=args.theta, adaptive=1, min_adaptive_dt=0.00333, max_pos_change=3.0,
-                               max_vel_change=3.0, device=local, autotune=1)
+    adaptive = dict(adaptive=1, min_adaptive_dt=0.00333, max_pos_change=3.0, max_vel_change=3.0)
+    params = nb.default_params(theta=args.theta, device=local, autotune=1, **adaptive)
     eng = nb.Engine(params)
     eng._lib.nbody_set_stream(eng._h, C_void(stream.cuda_stream))
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
-    # ---- resident steps (device-timed)
-    eng.set_particles(pos0, vel0, mass)
-    eng.step(args.warmup)
-    pos_w, vel_w = eng.get_particles()  # the e2e leg times the same K steps from this state
+    def initial_state_steps(e, steps, timed):
+        """`steps` single steps, each from the seeded initial state (restored and
+        L2 flushed outside the event pair). Returns (ms, interactions, launches)."""
+        ms = 0.0
+        inter = 0
+        launches = 0
+        for _ in range(steps):
+            e.set_particles(pos0, vel0, mass)
+            flush.fill_(1.0)
+            l0 = e.stats()["kernel_launches"]
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record(stream)
+            e.step(1)
+            b.record(stream)
+            torch.cuda.synchronize()
+            st = e.stats()
+            if timed:
+                ms += a.elapsed_time(b)
+                inter += st["interactions_total"]
+                launches += st["kernel_launches"] - l0
+        return ms, inter, launches
+
+    # ---- headline: K steps on the initial state, inputs resident (device-timed)
+    initial_state_steps(eng, args.warmup, False)  # autotune, graph capture, clocks up
     if pg:
         pg.barrier()
-    torch.cuda.synchronize()
-    launches0 = eng.stats()["kernel_launches"]
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(local) as clk:
-        ev0.record(stream)
-        eng.step(args.steps)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    st = eng.stats()
-    launches = st["kernel_launches"] - launches0
-    walk_shape = {"warps_per_block": st["walk_warps_per_block"], "blocks": st["walk_blocks"], "autotuned": True}
-    ms_total = ev0.elapsed_time(ev1)
-    inter_total = st["interactions_total"]
+        ms_total, inter_total, launches = initial_state_steps(eng, args.steps, True)
     ms_total, inter_all = job_totals(pg, "cuda", ms_total, inter_total)
     ms_step = ms_total / args.steps
     value = inter_all / (ms_total * 1e-3)
-    steps_per_s = 1e3 / ms_step
+    st = eng.stats()
+    walk_shape = {"warps_per_block": st["walk_warps_per_block"], "blocks": st["walk_blocks"], "autotuned": True}
 
-    # ---- per-phase times (CUDA events inside the engine, one step per call)
+    # ---- per-phase times on the initial state (CUDA events inside the engine)
     eng.set_timing(True)
     ph = {"tree": [], "com": [], "walk": [], "update": [], "inter": []}
     for _ in range(max(3, min(args.steps, 10))):
+        eng.set_particles(pos0, vel0, mass)
+        flush.fill_(1.0)
         eng.step(1)
-        s = eng.stats()
-        ph["tree"].append(s["ms_tree"]); ph["com"].append(s["ms_com"])
-        ph["walk"].append(s["ms_walk"]); ph["update"].append(s["ms_update"])
-        ph["inter"].append(s["interactions"])
+        s_ = eng.stats()
+        ph["tree"].append(s_["ms_tree"]); ph["com"].append(s_["ms_com"])
+        ph["walk"].append(s_["ms_walk"]); ph["update"].append(s_["ms_update"])
+        ph["inter"].append(s_["interactions"])
     eng.set_timing(False)
     walk_ms = float(np.mean(ph["walk"]))
     walk_inter = float(np.mean(ph["inter"]))
 
-    # ---- e2e: host buffers through the C ABI every step
+    # ---- e2e: host buffers through the C ABI, every step from the initial state
     hp = torch.empty((args.n, 3), dtype=torch.float64, pin_memory=True).numpy()
     hv = torch.empty((args.n, 3), dtype=torch.float64, pin_memory=True).numpy()
     hm = torch.empty((args.n,), dtype=torch.float64, pin_memory=True).numpy()
-    hp[:] = pos_w; hv[:] = vel_w; hm[:] = mass
+    hm[:] = mass
     for _ in range(max(1, args.warmup // 2)):
+        hp[:] = pos0; hv[:] = vel0
         eng.step_host(hp, hv, hm, 1)
-    hp[:] = pos_w; hv[:] = vel_w
+    if pg:
+        pg.barrier()
+    e2e_ms = 0.0
+    inter_e2e = 0
+    for _ in range(args.steps):
+        hp[:] = pos0; hv[:] = vel0
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        eng.step_host(hp, hv, hm, 1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+        inter_e2e += eng.stats()["interactions_total"]
+    e2e_ms, inter_e2e = job_totals(pg, "cuda", e2e_ms, inter_e2e)
+    e2e_value = float(inter_e2e) / (e2e_ms * 1e-3)
+
+    # ---- evolved (secondary): K consecutive steps of the collapsing shell
+    eng.set_particles(pos0, vel0, mass)
+    eng.step(args.warmup)
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    inter_e2e = 0
-    e0.record(stream)
-    for _ in range(args.steps):
-        eng.step_host(hp, hv, hm, 1)
-        inter_e2e += eng.stats()["interactions_total"]
-    e1.record(stream)
+    v0, v1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    v0.record(stream)
+    eng.step(args.steps)
+    v1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    e2e_ms, inter_e2e = job_totals(pg, "cuda", e2e_ms, inter_e2e)
-    e2e_value = float(inter_e2e) / (e2e_ms * 1e-3)
+    evo_ms, evo_inter = job_totals(pg, "cuda", v0.elapsed_time(v1), eng.stats()["interactions_total"])
+    evolved = {"value": evo_inter / (evo_ms * 1e-3), "unit": UNIT, "ms_per_step": evo_ms / args.steps,
+               "interactions_per_step": evo_inter / args.steps / world,
+               "steps": f"{args.steps} consecutive adaptive steps after {args.warmup} warm-up steps"}
 
     if rank != 0:
         eng.close()
@@ -295,42 +340,17 @@ def run_ours(args) -> None:
             pg.destroy_process_group()
         return
 
-    # ---- the plain FP64 form on the same workload, same initial state, same K.
+    # ---- the plain FP64 form on the same initial state, same protocol.
     # This and the legs below are single-GPU comparisons: under torchrun only the
     # headline runs, so rank 0 does not keep the other ranks waiting at the barrier.
-    fp64_ms_step = None
-    with nb.Engine(nb.default_params(theta=args.theta, adaptive=1, min_adaptive_dt=0.00333, max_pos_change=3.0,
-                                     max_vel_change=3.0, precision=nb.PRECISION_FP64, device=local)) as e64:
+    with nb.Engine(nb.default_params(theta=args.theta, precision=nb.PRECISION_FP64, device=local,
+                                     **adaptive)) as e64:
         e64._lib.nbody_set_stream(e64._h, C_void(stream.cuda_stream))
-        e64.set_particles(pos0, vel0, mass)
-        e64.step(args.warmup)
-        torch.cuda.synchronize()
-        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        f0.record(stream)
-        e64.step(args.steps)
-        f1.record(stream)
-        torch.cuda.synchronize()
-        fp64_ms_step = f0.elapsed_time(f1) / args.steps
+        initial_state_steps(e64, 3, False)
+        fp64_ms, _, _ = initial_state_steps(e64, args.steps, True)
+        fp64_ms_step = fp64_ms / args.steps
 
-    # ---- adjoint / forward at the adjoint configuration (sphere N=65536, K=256, checkpoint 16)
-    adjoint = None
-    if not args.no_adjoint and world == 1:
-        adjoint = adjoint_leg(nb, torch, stream, local, args.adjoint_fd)
-
-    # ---- batched ensemble (512 systems of uneven N, one persistent walk, graphs, autotuned)
-    ensemble = None
-    if not args.no_ensemble and world == 1:
-        ensemble = ensemble_leg(nb, torch, stream, local)
-
-    # ---- the other configurations: cube 5000 x 300 frames, sphere 100k x 100 steps, theta sweep at 1M
-    configs = None
-    if not args.no_configs and world == 1:
-        cube, cube_inputs = cube_leg(nb, torch, stream, local)
-        configs = {"cube5000": cube,
-                   "sphere100k": sphere_leg(nb, torch, stream, local),
-                   "shell1M_theta": theta_leg(nb, torch, stream, local, pos0, vel0, mass)}
-
-    # ---- accuracy on the initial state: vs the FP64 form (same lists) and FP64 direct sum
+    # ---- accuracy on the initial state: vs the FP64 form (same lists) and an FP64 direct sum
     acc_mixed, counts = eng.barnes_hut(pos0, mass, theta=args.theta, counts=True)
     with nb.Engine(nb.default_params(theta=args.theta, precision=nb.PRECISION_FP64, device=local)) as e64:
         acc64 = e64.barnes_hut(pos0, mass, theta=args.theta)
@@ -350,8 +370,28 @@ def run_ours(args) -> None:
     direct = {"p99_mixed": float(np.percentile(rel(acc_mixed[idx], d), 99)),
               "p99_fp64_bh": float(np.percentile(rel(acc64[idx], d), 99)),
               "sample": "4096 particles, numpy default_rng(0xDEADBEEF); nbody_direct_forces (FP64, compensated)"}
+    eng.close()
 
-    # ---- roofline of the fused walk kernel
+    # ---- adjoint / forward at the adjoint configuration (sphere N=65536, K=256, checkpoint 16)
+    adjoint = None
+    if not args.no_adjoint and world == 1:
+        adjoint = adjoint_leg(nb, torch, stream, local, args.adjoint_fd)
+
+    # ---- batched ensemble (512 systems of uneven N, one persistent walk, graphs, autotuned)
+    ensemble = None
+    if not args.no_ensemble and world == 1:
+        ensemble = ensemble_leg(nb, torch, stream, local)
+
+    # ---- the other configurations: cube 5000 x 300 frames, sphere 100k x 100 steps, theta sweep at 1M
+    configs = None
+    cube_inputs = None
+    if not args.no_configs and world == 1:
+        cube, cube_inputs = cube_leg(nb, torch, stream, local)
+        configs = {"cube5000": cube,
+                   "sphere100k": sphere_leg(nb, torch, stream, local),
+                   "shell1M_theta": theta_leg(nb, torch, stream, local, pos0, vel0, mass)}
+
+    # ---- roofline of the fused walk kernel (initial state)
     peak_tf, _ = nb.probe_fp32_peak(local)
     achieved = FLOP_PER_INTERACTION * walk_inter / (walk_ms * 1e-3) / 1e12
     # nominal FP32 peak for comparison: SMs x 128 lanes x 2 FLOP x the maximum SM clock
@@ -378,7 +418,7 @@ def run_ours(args) -> None:
             # the same measurement on one thread, for the per-core rate
             try:
                 v1, desc1, _, _ = cpu_reference_sample(pos0, mass, args.theta, min(args.cpu_seconds, 8.0), 1, counts)
-                cpu["single_thread"] = {"value": v1, "unit": UNIT, "cores": 1, "sample": desc1}
+                cpu["single_thread"] = {"value": v1, "unit": UNIT, "cores": 1}
             except Exception as ex:
                 cpu["single_thread"] = {"value": None, "sample": f"failed: {ex}"}
         if configs is not None:
@@ -387,53 +427,118 @@ def run_ours(args) -> None:
             except Exception as ex:  # the reference harness is only on boxes where it was built
                 configs["cube5000"]["cpu_baseline"] = {"unavailable": str(ex)}
 
+    details = {"phases_ms": {k: float(np.mean(v)) for k, v in ph.items() if k != "inter"},
+               "fp64_form_walk_ms": fp64_walk_ms, "vs_fp64_direct_sum": direct, "adjoint": adjoint,
+               "ensemble": ensemble, "configs": configs, "evolved": evolved, "walk_shape": walk_shape,
+               "cpu_baseline": cpu}
+    print("bench-details: " + json.dumps(details), flush=True)
+
+    fd = (adjoint or {}).get("fd_check") or {}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 pair forces + f64 tree/COM/state", "data": "synthetic (seeded reference generator)",
+        "vs_baseline": None, "dtype": "f32 pair forces + f64 tree/COM/state",
+        "data": "synthetic (seeded reference generator)",
         "config": workload_config(args),
-        "steps_per_s": steps_per_s * world,
+        "steps_per_s": 1e3 / ms_step * world,
         "interactions_per_step": inter_all / args.steps / world,
-        "phases_ms": {k: float(np.mean(v)) for k, v in ph.items() if k != "inter"},
+        "phases_ms": details["phases_ms"],
         "walk_interactions_per_s": walk_inter / (walk_ms * 1e-3),
-        "fp64_form_walk_ms": fp64_walk_ms,
+        "evolved": {k: evolved[k] for k in ("value", "ms_per_step", "interactions_per_step")},
         "fp64_form_ms_per_step": fp64_ms_step,
         "speedup_vs_fp64_form": fp64_ms_step / ms_step if fp64_ms_step else None,
         "p99_rel_err_vs_fp64_form": p99_vs_fp64,
-        "vs_fp64_direct_sum": direct,
+        "p99_rel_err_vs_fp64_direct_sum": direct["p99_mixed"],
         "adjoint_fwd_ratio": adjoint["ratio"] if adjoint else None,
-        "adjoint": adjoint,
-        "ensemble": ensemble,
-        "configs": configs,
+        "fd_check": {k: {q: v[q] for q in ("median_rel", "frac_le_1e-4")} for k, v in fd.items()
+                     if isinstance(v, dict) and "median_rel" in v} or None,
+        "ensemble_speedup_vs_sequential": ensemble["speedup_vs_sequential"] if ensemble else None,
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 56 * args.n,
                 "d2h_bytes_per_step": 48 * args.n},
         "gpu_launches": int(launches),
-        "walk_shape": walk_shape,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
                      "frac": achieved / peak_tf if peak_tf else None, "traffic": traffic,
-                     "kernel": "k_walk (fused walk + gravity)",
+                     "kernel": "k_walk (fused walk + gravity), initial state",
                      "peak_source": "measured FP32 FMA probe (nbody_probe_fp32_peak); MEASURED_PEAKS.json has no FP32 figure",
-                     "flop_per_interaction": FLOP_PER_INTERACTION,
-                     "peak_nominal": peak_nominal,
-                     "peak_nominal_basis": f"{sms} SMs x 128 FP32 lanes x 2 FLOP x {max_mhz} MHz (clocks.max.sm)"},
-        "cpu_baseline": cpu,
+                     "peak_nominal": peak_nominal},
+        "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
     }
     print(json.dumps(line), flush=True)
-    eng.close()
     if pg:
         pg.barrier()
         pg.destroy_process_group()
 
 
-def adjoint_leg(nb, torch, stream, device, fd_coords=0):
+def fd_coordinates(n, count, seed=0xDEADBEEF):
+    """Seeded coordinates for the finite-difference check: half positions, a
+    quarter velocities, a quarter masses, as (kind, particle, component)."""
+    rng = np.random.default_rng(seed)
+    npos, nvel = count // 2, count // 4
+    out = [("pos",) + divmod(int(q), 3) for q in rng.choice(3 * n, npos, replace=False)]
+    out += [("vel",) + divmod(int(q), 3) for q in rng.choice(3 * n, nvel, replace=False)]
+    out += [("mass", int(q), 0) for q in rng.choice(n, count - npos - nvel, replace=False)]
+    return out
+
+
+def fd_check(nb, e64, pos, vel, mass, target, K, coords, grads):
+    """FP64 central differences of the loss L = mean |x_K - target|^2 through
+    K fixed-dt steps of the FP64 form (decisions re-taken at every perturbed
+    state, as the reference would), eps = 1e-3 relative. Returns per-coordinate
+    finite differences and the relative errors of each gradient in `grads`."""
+    n = len(mass)
+    scale = {"pos": np.sqrt(np.mean(pos ** 2)), "vel": np.sqrt(np.mean(vel ** 2)), "mass": float(np.mean(mass))}
+    fds = []
+    for kind, p, k in coords:
+        arr = {"pos": pos, "vel": vel, "mass": mass}[kind]
+        v0 = arr[p, k] if kind != "mass" else arr[p]
+        h = 1e-3 * max(abs(v0), 1e-3 * scale[kind])
+        finals = []
+        for sgn in (1.0, -1.0):
+            x, v, m = pos.copy(), vel.copy(), mass.copy()
+            if kind == "pos":
+                x[p, k] += sgn * h
+            elif kind == "vel":
+                v[p, k] += sgn * h
+            else:
+                m[p] += sgn * h
+            e64.set_particles(x, v, m)
+            e64.step(K)
+            finals.append(e64.get_particles()[0])
+        xp, xm = finals
+        # L+ - L- as a sum of products of differences (no cancellation of two large losses)
+        dl = float(np.sum((xp - xm) * (xp + xm - 2.0 * target))) / n
+        fds.append(dl / (2 * h))
+    fds = np.array(fds)
+    out = {}
+    for name, (gp, gv, gm) in grads.items():
+        g = np.array([gp[p, k] if kind == "pos" else gv[p, k] if kind == "vel" else gm[p] for kind, p, k in coords])
+        rel = np.abs(fds - g) / np.maximum(np.maximum(np.abs(fds), np.abs(g)), 1e-300)
+        out[name] = {"median_rel": float(np.median(rel)), "max_rel": float(np.max(rel)),
+                     "frac_le_1e-4": float(np.mean(rel <= 1e-4)),
+                     "by_kind_median": {kd: float(np.median(rel[[c[0] == kd for c in coords]]))
+                                        for kd in ("pos", "vel", "mass")}}
+    return out
+
+
+def adjoint_leg(nb, torch, stream, device, fd_coords=64):
     """Config 4: sphere N=65536, theta 0.5, fixed dt 0.0333, K=256 steps,
     checkpoint every 16; loss = mean squared distance of the final positions to
-    a seeded Gaussian-perturbed (sigma 5) copy of the initial positions."""
+    a seeded Gaussian-perturbed (sigma 5) copy of the initial positions. Times
+    backward / forward (MIXED); compares the MIXED gradient with the FP64 form's;
+    checks both against FP64 central differences (eps 1e-3 relative) on
+    `fd_coords` seeded coordinates at K = 256 and at the short horizons K = 1, 4, 16."""
     n, K, every = 65536, 256, 16
     pos, vel, mass = nb.generate(n, gen_type=1, r_sphere=100.0, rotation_magnitude=0.1, seed=0xDEADBEEF)
     target = pos + np.random.default_rng(0xDEADBEEF).normal(0.0, 5.0, pos.shape)
     out = {"config": "sphere N=65536 theta=0.5 dt=0.0333 K=256 checkpoint 16", "precision": "mixed"}
+
+    def gradient(e, steps, ck):
+        e.set_particles(pos, vel, mass)
+        e.forward_checkpointed(steps, ck)
+        xK, _ = e.get_particles()
+        return e.backward(2.0 * (xK - target) / n), float(((xK - target) ** 2).sum() / n)
+
     with nb.Engine(nb.default_params(theta=0.5, dt=0.0333, device=device)) as e:
         e._lib.nbody_set_stream(e._h, C_void(stream.cuda_stream))
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
@@ -460,23 +565,34 @@ def adjoint_leg(nb, torch, stream, device, fd_coords=0):
                    loss=float(((xK - target) ** 2).sum() / n),
                    gradients_finite=bool(np.isfinite(gp).all() and np.isfinite(gv).all() and np.isfinite(gm).all()),
                    max_abs_dL_dpos0=float(np.abs(gp).max()))
+        mixed = {K: (gp, gv, gm)}
+        for k in (1, 4, 16):
+            mixed[k] = gradient(e, k, 0)[0]
+    with nb.Engine(nb.default_params(theta=0.5, dt=0.0333, precision=nb.PRECISION_FP64, device=device)) as e64:
+        e64._lib.nbody_set_stream(e64._h, C_void(stream.cuda_stream))
+        fp64 = {K: gradient(e64, K, every)[0]}
+        for k in (1, 4, 16):
+            fp64[k] = gradient(e64, k, 0)[0]
+        cmp = {}
+        for k in (1, 4, 16, K):
+            a = np.concatenate([x.ravel() for x in mixed[k]])
+            b = np.concatenate([x.ravel() for x in fp64[k]])
+            r = np.abs(a - b) / np.maximum(np.maximum(np.abs(a), np.abs(b)), 1e-300)
+            cmp[f"K{k}"] = {"median_rel": float(np.median(r)), "p99_rel": float(np.percentile(r, 99))}
+        out["mixed_vs_fp64_form_gradient"] = cmp
         if fd_coords:
-            rng = np.random.default_rng(0xDEADBEEF)
-            idx = rng.choice(3 * n, fd_coords, replace=False)
-            rel = []
-            for q in idx:
-                p, k = divmod(int(q), 3)
-                h = 1e-3 * max(abs(pos[p, k]), 1e-3)
-                vals = []
-                for sgn in (1, -1):
-                    x0 = pos.copy(); x0[p, k] += sgn * h
-                    e.set_particles(x0, vel, mass)
-                    e.step(K)
-                    vals.append(float(((e.get_particles()[0] - target) ** 2).sum() / n))
-                fd = (vals[0] - vals[1]) / (2 * h)
-                rel.append(abs(fd - gp[p, k]) / max(abs(fd), abs(gp[p, k]), 1e-300))
-            out["fd_check"] = {"coords": fd_coords, "eps": "1e-3 relative", "median_rel": float(np.median(rel)),
-                               "max_rel": float(np.max(rel)), "frac_le_1e-4": float(np.mean(np.array(rel) <= 1e-4))}
+            coords = fd_coordinates(n, fd_coords)
+            t0 = time.perf_counter()
+            checks = {}
+            for k in (1, 4, 16, K):
+                checks[f"K{k}"] = fd_check(nb, e64, pos, vel, mass, target, k,
+                                           coords, {"mixed": mixed[k], "fp64_form": fp64[k]})
+            fdc = {"coords": fd_coords, "eps": "1e-3 relative (of |value|, or of the array's RMS when larger)",
+                   "forward": "FP64 form, decisions re-taken at every perturbed state",
+                   "seconds": time.perf_counter() - t0}
+            for k, v in checks.items():
+                fdc[k] = dict(v["mixed"], fp64_form=v["fp64_form"])
+            out["fd_check"] = fdc
     return out
 
 
@@ -597,8 +713,14 @@ def ensemble_leg(nb, torch, stream, device, nsys=512, steps=100, seq_steps=10):
     [1024, 65536] (seeded), gen_type cycling cube/sphere/shell, masses uniform in
     [5e10, 5e11], theta 0.5, dt 0.0333, 100 steps: one engine, one persistent
     walk per step over all systems, steps replayed from a captured CUDA graph,
-    walk block shape autotuned. Baseline: the same systems stepped one after
-    another through one engine call each (graph replay too), seq_steps steps each."""
+    walk block shape autotuned.
+
+    Baseline: one engine per system, each with its particles already resident,
+    its walk shape autotuned on its own state and its step graph captured, all
+    outside the timed region; the timed region steps the systems one after
+    another, one engine call of seq_steps steps each, on the same stream. The
+    earlier baseline, which also uploaded each system inside the timed region,
+    is reported beside it (`sequential_with_uploads_*`)."""
     rng = np.random.default_rng(0xDEADBEEF)
     counts = np.exp(rng.uniform(np.log(1024), np.log(65536), nsys)).astype(np.uint32)
     parts = [nb.generate(int(c), gen_type=s % 3, size=512.0 if s % 3 == 0 else 1024.0, seed=0xDEADBEEF + s)
@@ -607,7 +729,7 @@ def ensemble_leg(nb, torch, stream, device, nsys=512, steps=100, seq_steps=10):
     mass = np.concatenate([p[2] for p in parts])
     out = {"systems": nsys, "particles": int(counts.sum()), "n_min": int(counts.min()), "n_max": int(counts.max()),
            "steps": steps, "theta": 0.5, "dt": 0.0333}
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
     with nb.Engine(nb.default_params(theta=0.5, dt=0.0333, device=device, autotune=1)) as e:
         e._lib.nbody_set_stream(e._h, C_void(stream.cuda_stream))
         e.set_systems(counts)
@@ -625,21 +747,46 @@ def ensemble_leg(nb, torch, stream, device, nsys=512, steps=100, seq_steps=10):
     out["ensemble_ms"] = ms
     out["ensemble_system_steps_per_s"] = nsys * steps / (ms * 1e-3)
     out["ensemble_interactions_per_s"] = inter / (ms * 1e-3)
+
+    # fair baseline: resident systems, tuned and captured beforehand
+    engines = []
+    try:
+        for p in parts:
+            es = nb.Engine(nb.default_params(theta=0.5, dt=0.0333, device=device, autotune=1))
+            engines.append(es)
+            es._lib.nbody_set_stream(es._h, C_void(stream.cuda_stream))
+            es.set_particles(p[0], p[1], p[2])
+            es.step(2)  # autotune on this system, capture its step graph
+        torch.cuda.synchronize()
+        ev[2].record(stream)
+        for es in engines:
+            es.step(seq_steps)
+        ev[3].record(stream)
+        torch.cuda.synchronize()
+        seq_ms = ev[2].elapsed_time(ev[3])
+    finally:
+        for es in engines:
+            es.close()
+    out["sequential_steps_per_system"] = seq_steps
+    out["sequential_system_steps_per_s"] = nsys * seq_steps / (seq_ms * 1e-3)
+    out["speedup_vs_sequential"] = out["ensemble_system_steps_per_s"] / out["sequential_system_steps_per_s"]
+
+    # the earlier baseline: one engine, each system uploaded inside the timed region
     with nb.Engine(nb.default_params(theta=0.5, dt=0.0333, device=device)) as e:
         e._lib.nbody_set_stream(e._h, C_void(stream.cuda_stream))
         e.set_particles(parts[0][0], parts[0][1], parts[0][2])
         e.step(2)
         torch.cuda.synchronize()
-        ev[2].record(stream)
+        ev[4].record(stream)
         for p in parts:
             e.set_particles(p[0], p[1], p[2])
             e.step(seq_steps)
-        ev[3].record(stream)
+        ev[5].record(stream)
         torch.cuda.synchronize()
-        seq_ms = ev[2].elapsed_time(ev[3])
-    out["sequential_steps_per_system"] = seq_steps
-    out["sequential_system_steps_per_s"] = nsys * seq_steps / (seq_ms * 1e-3)
-    out["speedup_vs_sequential"] = out["ensemble_system_steps_per_s"] / out["sequential_system_steps_per_s"]
+        up_ms = ev[4].elapsed_time(ev[5])
+    out["sequential_with_uploads_system_steps_per_s"] = nsys * seq_steps / (up_ms * 1e-3)
+    out["speedup_vs_sequential_with_uploads"] = out["ensemble_system_steps_per_s"] / out[
+        "sequential_with_uploads_system_steps_per_s"]
     return out
 
 

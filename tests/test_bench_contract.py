@@ -27,6 +27,8 @@ def test_reference_arm_line():
     assert d["steps"] == 2 and d["warmup"] == 1 and d["n_gpus"] == 1
     assert d["value"] > 0
     assert d["config"]["n"] == 20000 and d["config"]["workload"].startswith("shell N=20000")
+    # the reference's accepted nodes over every particle of the same initial state the GPU arm steps from
+    assert d["interactions_per_step"] > 20000 and "initial shell" in d["config"]["state"]
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["kind"] in ("reference", "port") and cb["cores"] >= 1
     assert "particles walked" in cb["sample"]
