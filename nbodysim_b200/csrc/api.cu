@@ -277,7 +277,8 @@ int copy_tree_slot(nbody_ctx *c, uint32_t i, bool save);
 
 int force_pass(nbody_ctx *c, int damping, double theta, bool fp64, bool want_vmax, bool track_amax,
                bool want_counts, bool want_pot, const double *pos = nullptr, bool adjoint = false,
-               const WalkLaunch *shape = nullptr, bool min_size = false, int save_slot = -1, int restore_slot = -1) {
+               const WalkLaunch *shape = nullptr, bool min_size = false, int save_slot = -1, int restore_slot = -1,
+               double *acc64_out = nullptr) {
     uint32_t n = c->n;
     unsigned launches = 1;
     NB_CUDA(launch_reset_pass(c->sc, c->stream));
@@ -323,7 +324,7 @@ int force_pass(nbody_ctx *c, int damping, double theta, bool fp64, bool want_vma
     a.damping = damping;
     a.single = single(c) ? 1 : 0;
     a.accf = fp64 ? nullptr : (float *)c->acc;
-    a.accd = fp64 ? (double *)c->acc : nullptr;
+    a.accd = fp64 ? (acc64_out ? acc64_out : (double *)c->acc) : nullptr;
     a.counts = want_counts ? c->counts : nullptr;
     a.pot = want_pot ? c->pot : nullptr;
     a.spill = c->spill;
@@ -350,7 +351,7 @@ int force_pass(nbody_ctx *c, int damping, double theta, bool fp64, bool want_vma
     }
     c->launches += launches;
     ev(c, 3);
-    c->have_acc = true;
+    if (!acc64_out) c->have_acc = true;
     return NBODY_OK;
 }
 
@@ -1238,7 +1239,11 @@ int nbody_get_diagnostics(nbody_ctx *c, nbody_diagnostics *out) {
     const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
     int rc = begin_call(c);
     if (rc) return rc;
-    rc = force_pass(c, c->p.damping, c->p.theta, fp64, false, false, false, true);
+    // The potentials come from the FP64 form of the walk in both precisions: the
+    // same opening decisions, FP64 pair terms and sums. A MIXED context keeps its
+    // accelerations; the pass writes its FP64 ones to scratch.
+    rc = force_pass(c, c->p.damping, c->p.theta, true, false, false, false, true, nullptr, false, nullptr, false, -1,
+                    -1, fp64 ? nullptr : c->acc_out);
     if (rc) return rc;
     ev(c, 4);
     NB_CUDA(launch_diag(c->pos, c->vel, c->mass, c->pot, c->n, c->diag_partial, kDiagBlocks, c->sc, c->stream));

@@ -18,11 +18,17 @@
 // MIXED precision: coordinates enter the inner loop as FP32 offsets from the
 // group's bbox centre, pair forces and accumulation are FP32. The opening test
 // r^2 < (side/theta)^2 is evaluated in FP32 with a proven error band; a lane
-// whose value falls inside the band re-evaluates the reference's FP64
-// expression exactly (side / sqrt(dx^2 + dy^2 + dz^2) > theta on the original
-// doubles), so decisions are those of the FP64 reference.
+// whose value falls inside the band re-evaluates the reference's expression
+// exactly (side / sqrt(dx^2 + dy^2 + dz^2) > theta on the original values, in
+// the arithmetic of the reference build: FP64, or the FLOAT build's float), so
+// decisions are those of the reference.
+// Accepted bodies go to one of three lists, each stored as pairs of entries
+// for the packed FP32 instructions (two entries per instruction): entries that
+// every lane of the group takes (no mask), entries some lanes take (a lane mask
+// each), and bodies close to the group's box, whose offsets carry an FP32
+// remainder so that close pairs keep FP32 accuracy of the offset itself.
 // FP64 ("plain form"): the same walk with every quantity in FP64 and the
-// reference's FP64 opening test evaluated directly.
+// reference's opening test evaluated directly.
 #include "walk.cuh"
 
 namespace nbody {
@@ -63,17 +69,31 @@ struct GroupConsts {
     uint32_t st[6];     // per-group statistics: entries, tiles, decisions, list, near, deepest stack
 };
 
+// MIXED lists of the forward walk are stored in pairs of entries, so that the
+// packed FP32 instructions (two lanes of arithmetic each) read their operands
+// straight from two 16-byte loads: entries 2j and 2j+1 occupy 8 floats
+// (x0, x1, y0, y1, z0, z1, Gm0, Gm1) at 8j. The adjoint keeps one float4 per entry.
 template <>
 struct WarpSmem<false> {
     GroupConsts gc;
     int2 stack[kStackCap];
     float4 tc[32];            // (com - ref).xyz, -
     float4 tq[32];            // q = (side/theta)^2, band half-width, reach mask bits, node ref bits
-    float4 lc[kListCap];      // (com - ref).xyz, G m
+    union {
+        float4 lc[kListCap];  // adjoint: (com - ref).xyz, G m per entry
+        float lp[4 * kListCap];  // forward: entries taken by some lanes, in pairs
+    };
+    float lf[4 * kListCap];   // forward: entries taken by every lane of the group, in pairs
     uint32_t lm[kListCap];
     int lr[kListCap];         // node refs (adjoint mode)
-    double4 nc[32];           // near list: com.xyz (absolute), G m
-    uint32_t nm[32];
+    union {
+        double4 nc[32];       // adjoint near list: com.xyz (absolute), G m
+        struct {
+            float hi[4 * kListCap];  // forward near list, in pairs: offsets rounded to FP32, G m
+            float lo[4 * kListCap];  // and what the rounding left (x, y, z; the fourth slot is 0)
+        } np;
+    };
+    uint32_t nm[kListCap];
     int nr[32];
 };
 
@@ -141,58 +161,107 @@ __device__ inline void spill_in(Sm &s, int &top, uint32_t &spill_top, const int2
     top = take;
 }
 
-// Gravity of the listed bodies on each lane's particle: a lane takes an entry
-// iff its bit is set in the entry's mask.
-template <bool kDamp>
-__device__ inline float pair_f32(float dx, float dy, float dz, float gm, float &inv) {
-    const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-    inv = rsqrt_ftz(r2);
-    if constexpr (kDamp) {
-        const float r = r2 * inv;
-        return gm * inv / (r2 + expf(-r));
-    } else {
-        return gm * inv * (inv * inv);
-    }
+// ---- packed FP32 pairs (sm_100 f32x2: one instruction, two FP32 lanes of work)
+__device__ inline uint64_t f2pack(float a, float b) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ inline void f2unpack(uint64_t r, float &a, float &b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r)); }
+__device__ inline uint64_t f2add(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ inline uint64_t f2mul(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ inline uint64_t f2fma(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
 }
 
-// The masked force loop: every lane computes every entry, a lane adds it iff
-// its bit (`bit`) is set in the entry's mask. Entries go in pairs into two
-// accumulator sets, which breaks the dependence chain of the sums.
-template <bool kDamp, bool kPot>
-__device__ inline void force_list_f32(const float4 *lc, const uint32_t *lm, int count, uint32_t bit, float px,
-                                      float py, float pz, float &ax, float &ay, float &az, float &pot) {
-    float bx = 0.f, by = 0.f, bz = 0.f, bp = 0.f;
-    int k = 0;
-#pragma unroll 4
-    for (; k + 1 < count; k += 2) {
-        const float4 c0 = lc[k], c1 = lc[k + 1];
-        const uint32_t m0 = lm[k], m1 = lm[k + 1];
-        const float dx0 = c0.x - px, dy0 = c0.y - py, dz0 = c0.z - pz;
-        const float dx1 = c1.x - px, dy1 = c1.y - py, dz1 = c1.z - pz;
-        float inv0, inv1;
-        const float f0 = pair_f32<kDamp>(dx0, dy0, dz0, c0.w, inv0);
-        const float f1 = pair_f32<kDamp>(dx1, dy1, dz1, c1.w, inv1);
-        if (m0 & bit) {
-            ax = fmaf(f0, dx0, ax); ay = fmaf(f0, dy0, ay); az = fmaf(f0, dz0, az);
-            if constexpr (kPot) pot = fmaf(c0.w, inv0, pot);
+// Writes entry k of a paired list.
+__device__ inline void put_pair_entry(float *l, int k, float x, float y, float z, float gm) {
+    float *e = l + 8 * (k >> 1) + (k & 1);
+    e[0] = x; e[2] = y; e[4] = z; e[6] = gm;
+}
+
+// An offset o (FP64) as hi + lo in FP32: hi = o rounded, lo = what it left, rounded.
+__device__ inline float lo_part(double o, float hi) { return (float)(o - (double)hi); }
+
+// Gravity of the entries of a paired list on this lane's particle, two entries
+// per packed instruction. kMasked: entry k is taken iff `bit` is set in lm[k];
+// an entry not taken enters with inverse distance 0, so it adds exactly 0 even
+// when it is the lane's own leaf (distance 0). Without kMasked every entry is
+// taken. An odd count is padded with a far, massless entry. Accumulates into
+// (ax, ay, az).
+//
+// kComp (the near list): the entry offsets are hi + lo pairs (`lo` holds the lo
+// parts in the same layout) and so is the particle's (plx, ply, plz): the
+// difference is (hi - phi) + (lo - plo). When hi and phi are within a factor
+// two of each other their difference is exact (Sterbenz), so a body close to
+// the particle gets its offset to FP32 accuracy of the offset itself.
+template <bool kDamp, bool kMasked, bool kComp = false>
+__device__ inline void force_pairs_f32(float *l, const uint32_t *lm, int count, uint32_t bit, float px, float py,
+                                       float pz, float &ax, float &ay, float &az, float *lo = nullptr,
+                                       float plx = 0.f, float ply = 0.f, float plz = 0.f) {
+    if (count & 1) {
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) {
+            put_pair_entry(l, count, 1e18f, 1e18f, 1e18f, 0.f);
+            if constexpr (kComp) put_pair_entry(lo, count, 0.f, 0.f, 0.f, 0.f);
         }
-        if (m1 & bit) {
-            bx = fmaf(f1, dx1, bx); by = fmaf(f1, dy1, by); bz = fmaf(f1, dz1, bz);
-            if constexpr (kPot) bp = fmaf(c1.w, inv1, bp);
-        }
+        __syncwarp();
     }
-    if (k < count) {
-        const float4 c = lc[k];
-        const float dx = c.x - px, dy = c.y - py, dz = c.z - pz;
-        float inv;
-        const float f = pair_f32<kDamp>(dx, dy, dz, c.w, inv);
-        if (lm[k] & bit) {
-            ax = fmaf(f, dx, ax); ay = fmaf(f, dy, ay); az = fmaf(f, dz, az);
-            if constexpr (kPot) pot = fmaf(c.w, inv, pot);
+    const uint64_t npx = f2pack(-px, -px), npy = f2pack(-py, -py), npz = f2pack(-pz, -pz);
+    uint64_t nlx = 0, nly = 0, nlz = 0;
+    if constexpr (kComp) { nlx = f2pack(-plx, -plx); nly = f2pack(-ply, -ply); nlz = f2pack(-plz, -plz); }
+    uint64_t sx = f2pack(0.f, 0.f), sy = sx, sz = sx;
+    const int pairs = (count + 1) >> 1;
+#pragma unroll 2
+    for (int j = 0; j < pairs; j++) {
+        const float4 A = *reinterpret_cast<const float4 *>(l + 8 * j);      // x0 x1 y0 y1
+        const float4 B = *reinterpret_cast<const float4 *>(l + 8 * j + 4);  // z0 z1 g0 g1
+        const float g0 = B.z, g1 = B.w;
+        uint64_t dx = f2add(f2pack(A.x, A.y), npx);
+        uint64_t dy = f2add(f2pack(A.z, A.w), npy);
+        uint64_t dz = f2add(f2pack(B.x, B.y), npz);
+        if constexpr (kComp) {
+            const float4 C = *reinterpret_cast<const float4 *>(lo + 8 * j);
+            const float4 D = *reinterpret_cast<const float4 *>(lo + 8 * j + 4);
+            dx = f2add(dx, f2add(f2pack(C.x, C.y), nlx));
+            dy = f2add(dy, f2add(f2pack(C.z, C.w), nly));
+            dz = f2add(dz, f2add(f2pack(D.x, D.y), nlz));
         }
+        const uint64_t r2 = f2fma(dz, dz, f2fma(dy, dy, f2mul(dx, dx)));
+        float r0, r1;
+        f2unpack(r2, r0, r1);
+        float i0 = rsqrt_ftz(r0), i1 = rsqrt_ftz(r1);
+        if constexpr (kMasked) {
+            const uint2 m = *reinterpret_cast<const uint2 *>(lm + 2 * j);
+            i0 = (m.x & bit) ? i0 : 0.f;
+            i1 = (m.y & bit) ? i1 : 0.f;
+        }
+        uint64_t f;
+        if constexpr (kDamp) {
+            const float q0 = r0 * i0, q1 = r1 * i1;
+            f = f2pack(g0 * i0 / (r0 + expf(-q0)), g1 * i1 / (r1 + expf(-q1)));
+        } else {
+            const uint64_t inv = f2pack(i0, i1);
+            f = f2mul(f2mul(f2mul(inv, inv), inv), f2pack(g0, g1));
+        }
+        sx = f2fma(f, dx, sx);
+        sy = f2fma(f, dy, sy);
+        sz = f2fma(f, dz, sz);
     }
-    ax += bx; ay += by; az += bz;
-    if constexpr (kPot) pot += bp;
+    float a0, a1;
+    f2unpack(sx, a0, a1); ax += a0 + a1;
+    f2unpack(sy, a0, a1); ay += a0 + a1;
+    f2unpack(sz, a0, a1); az += a0 + a1;
 }
 
 // Per-particle accepted-body counts of a list (only when counts are requested).
@@ -200,30 +269,6 @@ __device__ inline uint32_t count_list(const uint32_t *lm, int count, uint32_t bi
     uint32_t c = 0;
     for (int k = 0; k < count; k++) c += (lm[k] & bit) ? 1u : 0u;
     return c;
-}
-
-// Bodies too close to the group's box for FP32 offsets: each lane forms its
-// offset in FP64 from absolute coordinates, then runs the FP32 pair force.
-template <bool kDamp, bool kPot>
-__device__ inline void force_near_f32(const double4 *nc, const uint32_t *nm, int count, int lane, double bx,
-                                      double by, double bz, float &ax, float &ay, float &az, float &pot) {
-    for (int k = 0; k < count; k++) {
-        if (!((nm[k] >> lane) & 1u)) continue;
-        const double4 c = nc[k];
-        const float dx = (float)(c.x - bx), dy = (float)(c.y - by), dz = (float)(c.z - bz);
-        const float gm = (float)c.w;
-        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-        const float inv = rsqrt_ftz(r2);
-        float f;
-        if constexpr (kDamp) {
-            const float r = r2 * inv;
-            f = gm * inv / (r2 + expf(-r));
-        } else {
-            f = gm * inv * (inv * inv);
-        }
-        ax = fmaf(f, dx, ax); ay = fmaf(f, dy, ay); az = fmaf(f, dz, az);
-        if constexpr (kPot) pot = fmaf(gm, inv, pot);
-    }
 }
 
 // ---- adjoint pair terms (frozen decisions) --------------------------------
@@ -414,7 +459,7 @@ __device__ inline void force_list_f64(const double4 *lc, const uint32_t *lm, int
 template <bool kFp64, bool kDamp, bool kPot, bool kAdj, class Sm>
 __device__ inline void flush_list(Sm &s, int count, int lane, const WalkArgs &a, const double4 &b, float px, float py,
                                   float pz, double lax, double lay, double laz, float &fax, float &fay, float &faz,
-                                  float &fpot, double &dax, double &day, double &daz, double &dpot, uint32_t &cnt) {
+                                  double &dax, double &day, double &daz, double &dpot, uint32_t &cnt) {
     const uint32_t bit = 1u << lane;
     if constexpr (kAdj) {
         if constexpr (kFp64)
@@ -425,7 +470,7 @@ __device__ inline void flush_list(Sm &s, int count, int lane, const WalkArgs &a,
                                 faz, a.adj_node, a.adj_leaf);
     } else {
         if constexpr (kFp64) force_list_f64<kDamp, kPot>(s.lc, s.lm, count, lane, b.x, b.y, b.z, dax, day, daz, dpot);
-        else force_list_f32<kDamp, kPot>(s.lc, s.lm, count, bit, px, py, pz, fax, fay, faz, fpot);
+        else force_pairs_f32<kDamp, true>(s.lp, s.lm, count, bit, px, py, pz, fax, fay, faz);
     }
     if (a.counts) cnt += count_list(s.lm, count, bit);
 }
@@ -489,6 +534,8 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
         const double ry = 0.5 * (warp_min(b.y) + warp_max(b.y));
         const double rz = 0.5 * (warp_min(b.z) + warp_max(b.z));
         const float px = (float)(b.x - rx), py = (float)(b.y - ry), pz = (float)(b.z - rz);
+        // what the FP32 offsets left out (the forward near list adds it back)
+        const float plx = lo_part(b.x - rx, px), ply = lo_part(b.y - ry, py), plz = lo_part(b.z - rz, pz);
         // Error band of the FP32 opening test. With u = 2^-24 and Pm the largest
         // |offset| from the reference point in the group, every lane has
         // |r2_f32 - r2| <= 7.1u r2 + 7u Pm sqrt(r2) and |q_f32 - q| <= 1.01u q;
@@ -521,10 +568,10 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
             s.gc.pm_tol = pm_tol; s.gc.tiny = tiny; s.gc.near_r2 = near_r2;
             for (int q = 0; q < 6; q++) s.gc.st[q] = 0u;
         }
-        float fax = 0.f, fay = 0.f, faz = 0.f, fpot = 0.f;
+        float fax = 0.f, fay = 0.f, faz = 0.f;
         double dax = 0.0, day = 0.0, daz = 0.0, dpot = 0.0;
         uint32_t cnt = 0, nint = 0, nfallback = 0;
-        int top = 0, list_top = 0;
+        int top = 0, list_top = 0, full_top = 0, near_top = 0;
         uint32_t spill_top = 0;
         bool failed = false;
         if (root >= 0) {
@@ -700,31 +747,61 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                     near = r2box < s.gc.near_r2;
                 }
             }
-            const uint32_t am = __ballot_sync(FULL, accm != 0 && !near);
-            if (accm && !near) {
-                const int pos = list_top + __popc(am & lt);
-                if constexpr (kFp64) s.lc[pos] = make_double4(cx, cy, cz, kG * m);
-                else s.lc[pos] = make_float4(fcx, fcy, fcz, (float)(kG * m));
-                s.lm[pos] = accm;
-                if constexpr (kAdj) s.lr[pos] = ref;
+            if constexpr (!kFp64 && !kAdj) {
+                // entries every lane of the group takes go to a list without masks
+                const bool take = accm != 0 && !near;
+                const bool all = take && accm == vmask;
+                const uint32_t fmk = __ballot_sync(FULL, all);
+                const uint32_t pmk = __ballot_sync(FULL, take && !all);
+                const float gmf = (float)(kG * m);
+                if (all) {
+                    put_pair_entry(s.lf, full_top + __popc(fmk & lt), fcx, fcy, fcz, gmf);
+                } else if (take) {
+                    const int pos = list_top + __popc(pmk & lt);
+                    put_pair_entry(s.lp, pos, fcx, fcy, fcz, gmf);
+                    s.lm[pos] = accm;
+                }
+                full_top += __popc(fmk);
+                list_top += __popc(pmk);
+                if (lane == 0) s.gc.st[3] += __popc(fmk) + __popc(pmk);
+            } else {
+                const uint32_t am = __ballot_sync(FULL, accm != 0 && !near);
+                if (accm && !near) {
+                    const int pos = list_top + __popc(am & lt);
+                    if constexpr (kFp64) s.lc[pos] = make_double4(cx, cy, cz, kG * m);
+                    else s.lc[pos] = make_float4(fcx, fcy, fcz, (float)(kG * m));
+                    s.lm[pos] = accm;
+                    if constexpr (kAdj) s.lr[pos] = ref;
+                }
+                list_top += __popc(am);
+                if (lane == 0) s.gc.st[3] += __popc(am);
             }
-            list_top += __popc(am);
-            if (lane == 0) s.gc.st[3] += __popc(am);
-            if constexpr (!kFp64) {
+            if constexpr (!kFp64 && !kAdj) {
+                // forward: near bodies collect in their own paired list, offsets as hi + lo
+                const uint32_t nmk = __ballot_sync(FULL, near);
+                if (nmk) {
+                    if (near) {
+                        const int pos = near_top + __popc(nmk & lt);
+                        const double ox = cx - s.gc.ref[0], oy = cy - s.gc.ref[1], oz = cz - s.gc.ref[2];
+                        put_pair_entry(s.np.hi, pos, fcx, fcy, fcz, (float)(kG * m));
+                        put_pair_entry(s.np.lo, pos, lo_part(ox, fcx), lo_part(oy, fcy), lo_part(oz, fcz), 0.f);
+                        s.nm[pos] = accm;
+                    }
+                    near_top += __popc(nmk);
+                    if (lane == 0) s.gc.st[4] += __popc(nmk);
+                }
+            } else if constexpr (!kFp64) {
                 const uint32_t nmk = __ballot_sync(FULL, near);
                 if (nmk) {
                     if (near) {
                         const int pos = __popc(nmk & lt);
                         s.nc[pos] = make_double4(cx, cy, cz, kG * m);
                         s.nm[pos] = accm;
-                        if constexpr (kAdj) s.nr[pos] = ref;
+                        s.nr[pos] = ref;
                     }
                     __syncwarp();
-                    if constexpr (kAdj)
-                        adj_near_f32<kDamp>(s.nc, s.nm, s.nr, __popc(nmk), lane, b.x, b.y, b.z, (float)lax, (float)lay,
-                                            (float)laz, fax, fay, faz, a.adj_node, a.adj_leaf);
-                    else
-                        force_near_f32<kDamp, kPot>(s.nc, s.nm, __popc(nmk), lane, b.x, b.y, b.z, fax, fay, faz, fpot);
+                    adj_near_f32<kDamp>(s.nc, s.nm, s.nr, __popc(nmk), lane, b.x, b.y, b.z, (float)lax, (float)lay,
+                                        (float)laz, fax, fay, faz, a.adj_node, a.adj_leaf);
                     if (a.counts) cnt += count_list(s.nm, __popc(nmk), 1u << lane);
                     if (lane == 0) s.gc.st[4] += __popc(nmk);
                     __syncwarp();
@@ -760,18 +837,44 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
             }
             __syncwarp();
 
-            // ---- forces once the list is long enough
+            // ---- forces once a list is long enough
             if (list_top >= kListFlush) {
                 flush_list<kFp64, kDamp, kPot, kAdj>(s, list_top, lane, a, b, px, py, pz, lax, lay, laz, fax, fay, faz,
-                                                      fpot, dax, day, daz, dpot, cnt);
+                                                      dax, day, daz, dpot, cnt);
                 list_top = 0;
                 __syncwarp();
+            }
+            if constexpr (!kFp64 && !kAdj) {
+                if (full_top >= kListFlush) {
+                    force_pairs_f32<kDamp, false>(s.lf, nullptr, full_top, 0u, px, py, pz, fax, fay, faz);
+                    cnt += full_top;
+                    full_top = 0;
+                    __syncwarp();
+                }
+                if (near_top >= kListFlush) {
+                    force_pairs_f32<kDamp, true, true>(s.np.hi, s.nm, near_top, 1u << lane, px, py, pz, fax, fay, faz,
+                                                       s.np.lo, plx, ply, plz);
+                    if (a.counts) cnt += count_list(s.nm, near_top, 1u << lane);
+                    near_top = 0;
+                    __syncwarp();
+                }
             }
         }
         if (failed && lane == 0) atomicOr(&t.sc->status, kStatusCapacity);
         if (list_top > 0) {
-            flush_list<kFp64, kDamp, kPot, kAdj>(s, list_top, lane, a, b, px, py, pz, lax, lay, laz, fax, fay, faz, fpot,
+            flush_list<kFp64, kDamp, kPot, kAdj>(s, list_top, lane, a, b, px, py, pz, lax, lay, laz, fax, fay, faz,
                                                   dax, day, daz, dpot, cnt);
+        }
+        if constexpr (!kFp64 && !kAdj) {
+            if (full_top > 0) {
+                force_pairs_f32<kDamp, false>(s.lf, nullptr, full_top, 0u, px, py, pz, fax, fay, faz);
+                cnt += full_top;
+            }
+            if (near_top > 0) {
+                force_pairs_f32<kDamp, true, true>(s.np.hi, s.nm, near_top, 1u << lane, px, py, pz, fax, fay, faz,
+                                                   s.np.lo, plx, ply, plz);
+                if (a.counts) cnt += count_list(s.nm, near_top, 1u << lane);
+            }
         }
         __syncwarp();
 
@@ -794,7 +897,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
             }
             if (a.counts) a.counts[ui] = cnt;
             if constexpr (kPot) {
-                if (a.pot) a.pot[ui] = kFp64 ? -dpot : -(double)fpot;
+                if (a.pot) a.pot[ui] = -dpot;
             }
         }
         unsigned long long wc = nint;
@@ -818,9 +921,13 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
     }
 }
 
+// Potentials (diagnostics) are summed by the FP64 form only.
 template <bool kFp64, bool kAdj>
 const void *walk_kernel(int damping, bool pot) {
-    if constexpr (kAdj) {
+    if constexpr (!kFp64 && !kAdj) {
+        (void)pot;
+        return damping ? (const void *)k_walk<false, true, false, false> : (const void *)k_walk<false, false, false, false>;
+    } else if constexpr (kAdj) {
         return damping ? (const void *)k_walk<kFp64, true, false, true> : (const void *)k_walk<kFp64, false, false, true>;
     } else {
         if (damping)

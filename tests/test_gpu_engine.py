@@ -112,13 +112,26 @@ def test_diagnostics(nb, orc):
     assert np.allclose(d["momentum"], P, rtol=1e-10, atol=1e-10 * np.abs(mass[:, None] * vel).sum())
     assert np.allclose(d["angular_momentum"], L, rtol=1e-10)
     assert abs(d["mass"] - mass.sum()) <= 1e-12 * mass.sum()
-    # potential: mixed vs FP64 form, and vs direct-sum FP64 within the BH truncation
-    assert abs(d["potential"] - d64["potential"]) <= 1e-5 * abs(d64["potential"])
+    # potential: the MIXED form's diagnostics sum FP64 pair terms over the same lists as
+    # the FP64 form, so the two agree to FP64 rounding; vs direct-sum FP64 within the BH truncation
+    assert abs(d["potential"] - d64["potential"]) <= 1e-10 * abs(d64["potential"])
     G = 6.67384e-11
     r = np.linalg.norm(pos[:, None, :] - pos[None, :, :], axis=2)
     np.fill_diagonal(r, np.inf)
     pe = -0.5 * G * np.sum(mass[:, None] * mass[None, :] / r)
     assert abs(d64["potential"] - pe) <= 1e-2 * abs(pe)
+
+
+def test_diagnostics_keep_mixed_accelerations(nb):
+    """The FP64 potential pass of a MIXED context leaves its accelerations alone."""
+    pos, vel, mass = nb.generate(5000, gen_type=2, size=1024.0)
+    with nb.Engine() as e:
+        e.set_particles(pos, vel, mass)
+        e.compute_forces()
+        _, _, a0 = e.get_particles(acc=True)
+        d = e.diagnostics()
+        _, _, a1 = e.get_particles(acc=True)
+        assert np.array_equal(a0, a1) and np.isfinite(d["potential"]) and d["potential"] < 0
 
 
 def test_device_view(nb):
