@@ -9,6 +9,9 @@ constexpr int kWalkWarps = 4;       // default warps per block (the autotuner ma
 constexpr int kWalkMaxWarps = 4;    // largest block the walk kernel is compiled for
 constexpr int kStackCap = 640;      // shared-memory stack entries per warp
 constexpr int kSpillChunk = kStackCap / 2;
+// A tile pushes at most 32 lanes x 8 children; after a spill the stack must
+// still have room for all of them.
+static_assert(kStackCap - kSpillChunk >= 32 * 8, "a spill must leave room for one tile's pushes");
 constexpr int kListFlush = 32;      // force pass once the interaction list holds this many
 constexpr int kListCap = kListFlush + 32;
 
