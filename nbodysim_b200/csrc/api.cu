@@ -103,6 +103,10 @@ struct nbody_ctx {
     double *sys_root = nullptr;
     int32_t *sys_root_node = nullptr;
     bool single_pass = false;  // nbody_barnes_hut: one system regardless of the layout
+    // The last tree build found no equal first key words, so the next one sorts by
+    // the first word first (TreeBuild::first_word_sort); the build checks this
+    // itself and falls back to the full sort on the device when it is wrong.
+    bool first_word_sort = false;
     // CUDA graphs: one captured step replayed per step; per-offset graphs for the
     // adjoint's recompute and reverse steps. Rebuilt when their key changes.
     bool use_graphs = true;
@@ -242,6 +246,7 @@ int check_status(nbody_ctx *c) {
     s.last_dt = h.dt_used;
     for (int k = 0; k < 3; k++) s.root_center[k] = h.root_center[k];
     s.root_side = h.root_side;
+    c->first_word_sort = h.word_ties == 0;
     if (c->timing) {
         float ms[4] = {0, 0, 0, 0};
         for (int k = 0; k < 4; k++) cudaEventElapsedTime(&ms[k], c->ev[k], c->ev[k + 1]);
@@ -265,6 +270,7 @@ void tree_inputs(nbody_ctx *c, uint32_t n, bool want_vmax) {
     tb.vel_for_max = want_vmax ? c->vel : nullptr;
     tb.sc = c->sc;
     tb.single = single(c) ? 1 : 0;
+    tb.first_word_sort = c->first_word_sort ? 1 : 0;
 }
 
 void ev(nbody_ctx *c, int k) {
@@ -398,12 +404,14 @@ int download_acc(nbody_ctx *c, double *acc) {
 std::vector<unsigned char> graph_key(nbody_ctx *c, uint32_t extra) {
     struct K {
         uint32_t n, nsys, ngroups, extra;
+        int first_word;
         void *arena, *adj, *sys, *stream;
         nbody_params p;
         WalkLaunch wm, wf;
     } k;
     std::memset(&k, 0, sizeof k);
     k.n = c->n; k.nsys = c->nsys; k.ngroups = c->ngroups; k.extra = extra;
+    k.first_word = c->first_word_sort ? 1 : 0;
     k.arena = c->arena; k.adj = c->adj_arena; k.sys = c->sys_arena; k.stream = (void *)c->stream;
     k.p = c->p; k.wm = c->wl_mixed; k.wf = c->wl_fp64;
     const unsigned char *b = (const unsigned char *)&k;

@@ -53,6 +53,7 @@ struct DevScalars {
     uint32_t group_counter;
     uint32_t ticket;          // last-block tickets of reductions
     uint32_t deep_groups;
+    uint32_t word_ties;       // the last build found particles with equal first key words
     unsigned long long max_acc_bits;  // max |a| (non-negative double as ordered bits)
     unsigned long long max_vel_bits;  // max |v|
     double dt_used;

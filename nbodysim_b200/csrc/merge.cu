@@ -343,8 +343,8 @@ cudaError_t collide_fold(const MergeBufs &m, uint32_t k, const double *pos, cons
     uint64_t *kin = m.skey_a, *kout = m.skey_b;
     uint32_t *iin = m.sidx_a, *iout = m.sidx_b;
     for (int q = 0; q < 4; q++) {
-        e = sort_pass(kin, iin, kout, iout, k, q, 8 * q, m.sort_scratch, &m.counters[kMcStatus], kMergeStatusSort, st,
-                      launches);
+        e = sort_pass(kin, iin, kout, iout, k, q, q, 8 * q, m.sort_scratch, &m.counters[kMcStatus], kMergeStatusSort,
+                      nullptr, st, launches);
         if (e != cudaSuccess) return e;
         uint64_t *tk = kin; kin = kout; kout = tk;
         uint32_t *ti = iin; iin = iout; iout = ti;

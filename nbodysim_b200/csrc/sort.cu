@@ -69,13 +69,15 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint64_t *__restric
                                                        const uint32_t *__restrict__ iin, uint64_t *__restrict__ kout,
                                                        uint32_t *__restrict__ iout, uint32_t n, int shift,
                                                        const uint32_t *__restrict__ goff, uint32_t *status,
-                                                       uint32_t *ticket, uint32_t *err, uint32_t err_bit) {
+                                                       uint32_t *ticket, uint32_t *err, uint32_t err_bit,
+                                                       const uint32_t *run_if) {
     __shared__ uint32_t s_wc[kWarps][256];  // per-warp digit counts, then per-warp offsets
     __shared__ uint32_t s_base[256];        // global position of the tile's first key of each digit
     __shared__ uint32_t s_lstart[256];      // position of each digit's first key within the tile
     __shared__ uint32_t s_wsum[kWarps];
     __shared__ uint64_t s_buf[kTile];       // the tile in digit order: keys, then indices
     __shared__ uint32_t s_tile;
+    if (run_if && *run_if == 0u) return;  // a pass that runs only when a device-side flag is set
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     if (t == 0) s_tile = atomicAdd(ticket, 1u);
     for (int k = 0; k < kWarps; k++) s_wc[k][t] = 0;
@@ -204,15 +206,19 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint64_t *__restric
 
 }  // namespace
 
+// Scratch: the digit offsets of up to 18 passes (histogram slots), then the
+// tile status words and the ticket of up to kPassSlots passes.
+constexpr int kHistSlots = 18;
+constexpr int kPassSlots = 26;
+
 size_t sort_scratch_bytes(uint32_t n) {
     const size_t tiles = (n + kTile - 1) / kTile;
-    return 4 * (18 * 256 + 18 * tiles * 256 + 32);
+    return 4 * (kHistSlots * 256 + kPassSlots * tiles * 256 + 32);
 }
 
 cudaError_t sort_prepare(const uint64_t *w0, const uint64_t *w1, const uint32_t *w2, uint32_t n, int npass,
                          uint32_t *scratch, cudaStream_t st, unsigned *launches) {
-    const size_t tiles = (n + kTile - 1) / kTile;
-    cudaError_t e = cudaMemsetAsync(scratch, 0, 4 * (18 * 256 + 18 * tiles * 256 + 32), st);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, sort_scratch_bytes(n), st);
     if (e != cudaSuccess) return e;
     const unsigned blocks = (unsigned)std::min<size_t>(1184, (n + 255) / 256);
     k_hist_all<<<blocks ? blocks : 1, 256, 0, st>>>(w0, w1, w2, n, npass, scratch);
@@ -222,14 +228,14 @@ cudaError_t sort_prepare(const uint64_t *w0, const uint64_t *w1, const uint32_t 
 }
 
 cudaError_t sort_pass(const uint64_t *kin, const uint32_t *iin, uint64_t *kout, uint32_t *iout, uint32_t n, int pass,
-                      int shift, uint32_t *scratch, uint32_t *err, uint32_t err_bit, cudaStream_t st,
-                      unsigned *launches) {
+                      int slot, int shift, uint32_t *scratch, uint32_t *err, uint32_t err_bit, const uint32_t *run_if,
+                      cudaStream_t st, unsigned *launches) {
     const size_t tiles = (n + kTile - 1) / kTile;
     uint32_t *goff = scratch + 256 * pass;
-    uint32_t *status = scratch + 18 * 256 + (size_t)pass * tiles * 256;
-    uint32_t *ticket = scratch + 18 * 256 + 18 * tiles * 256 + pass;
+    uint32_t *status = scratch + kHistSlots * 256 + (size_t)slot * tiles * 256;
+    uint32_t *ticket = scratch + kHistSlots * 256 + kPassSlots * tiles * 256 + slot;
     k_onesweep<<<(unsigned)tiles, kThreads, 0, st>>>(kin, iin, kout, iout, n, shift, goff, status, ticket, err,
-                                                     err_bit);
+                                                     err_bit, run_if);
     *launches += 1;
     return cudaGetLastError();
 }

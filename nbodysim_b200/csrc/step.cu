@@ -118,6 +118,7 @@ __global__ void k_reset_pass(DevScalars *sc) {
     sc->group_counter = 0;
     sc->ticket = 0;
     sc->deep_groups = 0;
+    sc->word_ties = 0;
     sc->max_acc_bits = 0;
     sc->max_vel_bits = 0;
 }

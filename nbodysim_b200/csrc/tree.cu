@@ -186,7 +186,8 @@ __device__ inline void descend_words(const double *p, const double *root, int wo
 __global__ void k_keys(const double *__restrict__ pos, uint32_t n, const DevScalars *sc,
                        uint64_t *__restrict__ k1_user, uint64_t *__restrict__ k2_sortkey,
                        uint64_t *__restrict__ k2_user, uint32_t *__restrict__ idx,
-                       const uint32_t *__restrict__ sys_id, const double *__restrict__ sys_root, int single) {
+                       const uint32_t *__restrict__ sys_id, const double *__restrict__ sys_root, int single,
+                       int sort_by_k1) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double root[4];
@@ -202,15 +203,36 @@ __global__ void k_keys(const double *__restrict__ pos, uint32_t n, const DevScal
     if (single) descend_words<float>(p, root, 2, w);
     else descend_words<double>(p, root, 2, w);
     k1_user[i] = w[0];
-    k2_sortkey[i] = w[1];
+    k2_sortkey[i] = sort_by_k1 ? w[0] : w[1];
     k2_user[i] = w[1];
     idx[i] = i;
 }
 
+// dst[j] = src[idx[j]]; with run_if non-null, only when *run_if is non-zero.
 __global__ void k_gather_key(const uint64_t *__restrict__ src, const uint32_t *__restrict__ idx,
-                             uint64_t *__restrict__ dst, uint32_t n) {
+                             uint64_t *__restrict__ dst, uint32_t n, const uint32_t *run_if) {
+    if (run_if && *run_if == 0u) return;
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j < n) dst[j] = src[idx[j]];
+}
+
+// Flags equal neighbours among the sorted first key words: then the first 21
+// octree levels do not separate every particle and the second word is needed.
+__global__ void k_word_ties(const uint64_t *__restrict__ k1_sorted, uint32_t n, uint32_t *ties) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool tie = j + 1 < n && k1_sorted[j] == k1_sorted[j + 1];
+    if (__any_sync(0xffffffffu, tie) && (threadIdx.x & 31) == 0) atomicOr(ties, 1u);
+}
+
+// Start of the full sort after ties: the second words as sort keys, identity indices.
+__global__ void k_full_sort_init(const uint64_t *__restrict__ k2_user, uint64_t *__restrict__ key,
+                                 uint32_t *__restrict__ idx, uint32_t n, const uint32_t *run_if) {
+    if (*run_if == 0u) return;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        key[i] = k2_user[i];
+        idx[i] = i;
+    }
 }
 
 __global__ void k_gather_sys(const uint32_t *__restrict__ sys_id, const uint32_t *__restrict__ idx,
@@ -629,37 +651,62 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
         k_bbox_systems<<<tb.nsys, 256, 0, st>>>(tb.pos, tb.mass, tb.sys_start, tb.sys_root, tb.sc, tb.single);
         L += 1;
     }
-    // keys: k1 (user order) -> key3, k2 -> key_a (sort key) and key2 (user order)
-    k_keys<<<blocks_for(n, 256), 256, 0, st>>>(tb.pos, n, tb.sc, tb.key3, tb.key_a, tb.key2, tb.idx_a,
-                                               multi ? tb.sys_id : nullptr, tb.sys_root, tb.single);
-    L += 2;
-    // LSD radix sort by (system, k1, k2): 8 passes on k2, 8 on k1, 2 on the system id.
-    cudaError_t e = sort_prepare(tb.key2, tb.key3, multi ? tb.sys_id : nullptr, n, multi ? 18 : 16, tb.sort_scratch,
-                                 st, &L);
-    if (e != cudaSuccess) return e;
     uint32_t *sort_err = &tb.sc->status;
-    auto passes = [&](uint64_t *kin, uint64_t *kout, uint32_t *iin, uint32_t *iout, int first, int count) {
+    uint32_t *ties = &tb.sc->word_ties;
+    // one LSD pass sequence: count passes ping-ponging kin/kout and iin/iout (an
+    // even count leaves the result in kin/iin), histogram passes from `first`,
+    // status slots from `slot`
+    auto passes = [&](uint64_t *kin, uint64_t *kout, uint32_t *iin, uint32_t *iout, int first, int slot, int count,
+                      const uint32_t *run_if) {
         for (int q = 0; q < count; q++) {
-            sort_pass(kin, iin, kout, iout, n, first + q, 8 * q, tb.sort_scratch, sort_err, kStatusSortStall, st, &L);
+            sort_pass(kin, iin, kout, iout, n, first + q, slot + q, 8 * q, tb.sort_scratch, sort_err, kStatusSortStall,
+                      run_if, st, &L);
             uint64_t *tk = kin; kin = kout; kout = tk;
             uint32_t *ti = iin; iin = iout; iout = ti;
         }
     };
-    passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b, 0, 8);    // result: key_a, idx_a
-    k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key3, tb.idx_a, tb.key_b, n);  // k1 in that order
-    passes(tb.key_b, tb.key_a, tb.idx_a, tb.idx_b, 8, 8);    // result: key_b (k1 sorted), idx_a
+    const bool first_word = tb.first_word_sort && !multi;
+    // keys: k1 (user order) -> key3, k2 (user order) -> key2; the sort key is k2
+    // (key_a) or, sorting by the first word first, k1 (key_b)
+    k_keys<<<blocks_for(n, 256), 256, 0, st>>>(tb.pos, n, tb.sc, tb.key3, first_word ? tb.key_b : tb.key_a, tb.key2,
+                                               tb.idx_a, multi ? tb.sys_id : nullptr, tb.sys_root, tb.single,
+                                               first_word ? 1 : 0);
+    L += 2;
+    // Histograms: passes 0-7 by the bytes of k2, 8-15 of k1, 16-17 of the system id.
+    cudaError_t e = sort_prepare(tb.key2, tb.key3, multi ? tb.sys_id : nullptr, n, multi ? 18 : 16, tb.sort_scratch,
+                                 st, &L);
+    if (e != cudaSuccess) return e;
+    if (first_word) {
+        // Sort by k1 alone (8 passes). When every k1 differs, that is the order by
+        // (k1, k2); a tie anywhere sets the flag and the full sort below runs.
+        passes(tb.key_b, tb.key_a, tb.idx_a, tb.idx_b, 8, 18, 8, nullptr);  // result: key_b (k1 sorted), idx_a
+        k_word_ties<<<blocks_for(n, 256), 256, 0, st>>>(tb.key_b, n, ties);
+        k_full_sort_init<<<blocks_for(n, 256), 256, 0, st>>>(tb.key2, tb.key_a, tb.idx_a, n, ties);
+        L += 2;
+    }
+    // LSD radix sort by (system, k1, k2): 8 passes on k2, 8 on k1, 2 on the system id
+    // (after the first-word sort: only when it found ties).
+    const uint32_t *run_if = first_word ? ties : nullptr;
+    passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b, 0, 0, 8, run_if);    // result: key_a, idx_a
+    k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key3, tb.idx_a, tb.key_b, n, run_if);  // k1 in that order
+    passes(tb.key_b, tb.key_a, tb.idx_a, tb.idx_b, 8, 8, 8, run_if);    // result: key_b (k1 sorted), idx_a
+    L += 1;
     if (multi) {
         // then by system (16-bit ids, 2 stable passes; result back in key_a / idx_a)
         k_gather_sys<<<blocks_for(n, 256), 256, 0, st>>>(tb.sys_id, tb.idx_a, tb.key_a, nullptr, n);
-        passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b, 16, 2);
-        k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key3, tb.idx_a, tb.key_b, n);  // k1 sorted
+        passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b, 16, 16, 2, nullptr);
+        k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key3, tb.idx_a, tb.key_b, n, nullptr);  // k1 sorted
         k_gather_sys<<<blocks_for(n, 256), 256, 0, st>>>(tb.sys_id, tb.idx_a, nullptr, tb.sys_sorted, n);
         L += 3;
+    } else if (!first_word) {
+        // tell the host whether the next build may sort by the first word first
+        k_word_ties<<<blocks_for(n, 256), 256, 0, st>>>(tb.key_b, n, ties);
+        L += 1;
     }
-    k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key2, tb.idx_a, tb.key_a, n);  // k2 sorted
+    k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key2, tb.idx_a, tb.key_a, n, nullptr);  // k2 sorted
     if (tb.mass_ready && !multi) cudaStreamWaitEvent(st, tb.mass_ready, 0);  // the first reader of the masses
     k_gather_bodies<<<blocks_for(n, 256), 256, 0, st>>>(tb.idx_a, tb.pos, tb.mass, tb.body, n, tb.sc, tb.single);
-    L += 3;
+    L += 2;
     *launches += L;
     if (n < 2) return cudaGetLastError();
     L = 0;

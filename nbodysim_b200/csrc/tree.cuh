@@ -13,6 +13,9 @@ struct TreeBuild {
                                 // the build waits for this event before it first reads them
     const double *vel_for_max;  // non-null: also reduce max |v| (adaptive dt)
     int keep_root;              // rebuild inside the root cube already in sc (single system)
+    int first_word_sort;        // sort by the first key word (levels 1-21) first, and run the full
+                                // two-word sort only when that leaves ties (sc->word_ties); single
+                                // system only. The result is the same either way.
     int single;                 // the reference's FLOAT build: positions and masses are read as
                                 // floats; root cube, child centres, node masses and centres of
                                 // mass are computed in float arithmetic

@@ -229,3 +229,98 @@ def test_backward_at_full_scale_independent_of_checkpoints(nb, precision):
     tol = 1e-6 if precision == 1 else 1e-5
     for a, b in zip(grads[1], grads[0]):
         assert np.abs(a - b).max() <= tol * np.abs(b).max(), np.abs(a - b).max() / np.abs(b).max()
+
+
+# ---- config 4 (sphere N = 65,536, theta 0.5, dt 0.0333) against central differences ----
+
+def _config4(nb):
+    n = 65536
+    pos, vel, mass = nb.generate(n, gen_type=1, r_sphere=100.0, rotation_magnitude=0.1, seed=0xDEADBEEF)
+    target = pos + np.random.default_rng(0xDEADBEEF).normal(0.0, 5.0, pos.shape)
+    return pos, vel, mass, target
+
+
+def _coords(n, count, seed=0xDEADBEEF):
+    rng = np.random.default_rng(seed)
+    out = [("pos",) + divmod(int(q), 3) for q in rng.choice(3 * n, count // 2, replace=False)]
+    out += [("vel",) + divmod(int(q), 3) for q in rng.choice(3 * n, count // 4, replace=False)]
+    out += [("mass", int(q), 0) for q in rng.choice(n, count - count // 2 - count // 4, replace=False)]
+    return out
+
+
+def _central_difference(e, pos, vel, mass, target, K, kind, p, k, h, count_flips=False):
+    """FP64 central difference of L = mean |x_K - target|^2 (L+ - L- summed as
+    products of differences), and the particles whose accepted-node count
+    differed from the unperturbed run, summed over the K steps of both runs."""
+    n = len(mass)
+    finals, flips = [], 0
+    for sgn in (1.0, -1.0):
+        x, v, m = pos.copy(), vel.copy(), mass.copy()
+        if kind == "pos":
+            x[p, k] += sgn * h
+        elif kind == "vel":
+            v[p, k] += sgn * h
+        else:
+            m[p] += sgn * h
+        bx, bv = pos.copy(), vel.copy()
+        for _ in range(K):
+            if count_flips:
+                _, cb = e.barnes_hut(bx, mass, theta=0.5, counts=True)
+                _, cp = e.barnes_hut(x, m, theta=0.5, counts=True)
+                flips += int((cb != cp).sum())
+                e.set_particles(bx, bv, mass); e.step(1); bx, bv = e.get_particles()
+            e.set_particles(x, v, m); e.step(1); x, v = e.get_particles()
+        finals.append(x)
+    xp, xm = finals
+    return float(np.sum((xp - xm) * (xp + xm - 2.0 * target))) / n / (2 * h), flips
+
+
+def test_config4_one_step_matches_central_differences(nb):
+    """K = 1 at config 4's size: steps of 1e-6 of each position or velocity (1e-3
+    of each mass, where the loss moves far less) flip no opening decision, and
+    the adjoint agrees with the FP64 central differences on 24 seeded coordinates:
+    FP64 form to 1e-5, MIXED form to 1e-4 relative."""
+    pos, vel, mass, target = _config4(nb)
+    n = len(mass)
+    scale = {"pos": np.sqrt(np.mean(pos ** 2)), "vel": np.sqrt(np.mean(vel ** 2)), "mass": float(np.mean(mass))}
+    grads = {}
+    for prec in (nb.PRECISION_FP64, nb.PRECISION_MIXED):
+        with nb.Engine(precision=prec, theta=0.5, dt=0.0333) as e:
+            e.set_particles(pos, vel, mass)
+            e.forward_checkpointed(1, 0)
+            x1, _ = e.get_particles()
+            grads[prec] = e.backward(2.0 * (x1 - target) / n)
+    with nb.Engine(precision=nb.PRECISION_FP64, theta=0.5, dt=0.0333) as e64:
+        for kind, p, k in _coords(n, 24):
+            arr = {"pos": pos, "vel": vel, "mass": mass}[kind]
+            v0 = arr[p] if kind == "mass" else arr[p, k]
+            h = (1e-3 if kind == "mass" else 1e-6) * max(abs(v0), 1e-3 * scale[kind])
+            fd, flips = _central_difference(e64, pos, vel, mass, target, 1, kind, p, k, h, count_flips=True)
+            assert flips == 0, (kind, p, k, flips)
+            for prec, tol in ((nb.PRECISION_FP64, 1e-5), (nb.PRECISION_MIXED, 1e-4)):
+                gp, gv, gm = grads[prec]
+                g = gm[p] if kind == "mass" else (gp if kind == "pos" else gv)[p, k]
+                assert abs(fd - g) <= tol * max(abs(fd), abs(g)), (prec, kind, p, k, fd, g)
+
+
+def test_config4_central_differences_ill_conditioned_beyond_one_step(nb):
+    """From the second step on, the unsoftened sphere's close encounters make the
+    loss a badly conditioned function of the initial state: particles that pass
+    within ~1e-4 of each other are thrown thousands of units (max |x_2| ~ 5e3),
+    and rounding-level differences between two runs are amplified by the
+    encounter. Central differences then depend on their own step size by more
+    than the 1e-4 bar: here, at K = 2 and 4, the quotients with steps of 1e-4
+    and 1e-6 of |x| differ by more than 1e-3 for most position coordinates, so a
+    finite-difference check of the adjoint cannot be decided at that bar beyond
+    K = 1 (the one-step test above decides it)."""
+    pos, vel, mass, target = _config4(nb)
+    n = len(mass)
+    coords = [c for c in _coords(n, 24) if c[0] == "pos"][:6]
+    with nb.Engine(precision=nb.PRECISION_FP64, theta=0.5, dt=0.0333) as e64:
+        for K in (2, 4):
+            unstable = 0
+            for kind, p, k in coords:
+                a, _ = _central_difference(e64, pos, vel, mass, target, K, kind, p, k, 1e-4 * abs(pos[p, k]))
+                b, _ = _central_difference(e64, pos, vel, mass, target, K, kind, p, k, 1e-6 * abs(pos[p, k]))
+                unstable += abs(a - b) > 1e-3 * max(abs(a), abs(b))
+            assert unstable >= len(coords) // 2, (K, unstable)
