@@ -131,6 +131,8 @@ struct nbody_ctx {
     size_t direct_bytes = 0;
     // nbody_step_host: masses and velocities uploaded on a second stream while the tree is built
     cudaStream_t aux_stream = nullptr;
+    // captures the tree build's full sort into a conditional graph node
+    cudaStream_t cond_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_mass = nullptr, ev_vel = nullptr;
     cudaEvent_t mass_pending = nullptr;  // set while a force pass must wait for ev_mass before reading masses
 };
@@ -271,6 +273,7 @@ void tree_inputs(nbody_ctx *c, uint32_t n, bool want_vmax) {
     tb.sc = c->sc;
     tb.single = single(c) ? 1 : 0;
     tb.first_word_sort = c->first_word_sort ? 1 : 0;
+    tb.cond_stream = c->cond_stream;
 }
 
 void ev(nbody_ctx *c, int k) {
@@ -913,6 +916,8 @@ int nbody_create(const nbody_params *p, nbody_ctx **out) {
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
         return cleanup(fail(NBODY_ERR_CUDA, "stream creation failed%s"));
     c->own_stream = true;
+    if (cudaStreamCreateWithFlags(&c->cond_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return cleanup(fail(NBODY_ERR_CUDA, "stream creation failed%s"));
     if (cudaMalloc(&c->sc, sizeof(DevScalars)) != cudaSuccess) return cleanup(fail(NBODY_ERR_OOM, "scalars%s"));
     if (cudaMemset(c->sc, 0, sizeof(DevScalars)) != cudaSuccess) return cleanup(fail(NBODY_ERR_CUDA, "memset%s"));
     if (cudaMallocHost(&c->hsc, sizeof(DevScalars)) != cudaSuccess) return cleanup(fail(NBODY_ERR_OOM, "pinned%s"));
@@ -951,6 +956,7 @@ int nbody_destroy(nbody_ctx *c) {
     if (c->pairs) cudaFree(c->pairs);
     if (c->hcounters) cudaFreeHost(c->hcounters);
     if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
+    if (c->cond_stream) cudaStreamDestroy(c->cond_stream);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_mass) cudaEventDestroy(c->ev_mass);
     if (c->ev_vel) cudaEventDestroy(c->ev_vel);

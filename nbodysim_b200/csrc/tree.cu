@@ -218,10 +218,16 @@ __global__ void k_gather_key(const uint64_t *__restrict__ src, const uint32_t *_
 
 // Flags equal neighbours among the sorted first key words: then the first 21
 // octree levels do not separate every particle and the second word is needed.
-__global__ void k_word_ties(const uint64_t *__restrict__ k1_sorted, uint32_t n, uint32_t *ties) {
+// Inside a captured graph (use_cond) it also sets the condition of the graph
+// node that holds the full sort.
+__global__ void k_word_ties(const uint64_t *__restrict__ k1_sorted, uint32_t n, uint32_t *ties,
+                            cudaGraphConditionalHandle cond, int use_cond) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     const bool tie = j + 1 < n && k1_sorted[j] == k1_sorted[j + 1];
-    if (__any_sync(0xffffffffu, tie) && (threadIdx.x & 31) == 0) atomicOr(ties, 1u);
+    if (__any_sync(0xffffffffu, tie) && (threadIdx.x & 31) == 0) {
+        atomicOr(ties, 1u);
+        if (use_cond) cudaGraphSetConditional(cond, 1u);
+    }
 }
 
 // Start of the full sort after ties: the second words as sort keys, identity indices.
@@ -657,13 +663,21 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
     // even count leaves the result in kin/iin), histogram passes from `first`,
     // status slots from `slot`
     auto passes = [&](uint64_t *kin, uint64_t *kout, uint32_t *iin, uint32_t *iout, int first, int slot, int count,
-                      const uint32_t *run_if) {
+                      const uint32_t *run_if, cudaStream_t s) {
         for (int q = 0; q < count; q++) {
             sort_pass(kin, iin, kout, iout, n, first + q, slot + q, 8 * q, tb.sort_scratch, sort_err, kStatusSortStall,
-                      run_if, st, &L);
+                      run_if, s, &L);
             uint64_t *tk = kin; kin = kout; kout = tk;
             uint32_t *ti = iin; iin = iout; iout = ti;
         }
+    };
+    // the LSD sort by (k1, k2) on stream `s`: 8 passes on k2, the gather of k1, 8
+    // passes on k1 (result: key_b sorted by k1, idx_a)
+    auto full_sort = [&](cudaStream_t s, const uint32_t *run_if) {
+        passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b, 0, 0, 8, run_if, s);    // result: key_a, idx_a
+        k_gather_key<<<blocks_for(n, 256), 256, 0, s>>>(tb.key3, tb.idx_a, tb.key_b, n, run_if);  // k1 in that order
+        passes(tb.key_b, tb.key_a, tb.idx_a, tb.idx_b, 8, 8, 8, run_if, s);    // result: key_b (k1 sorted), idx_a
+        L += 1;
     };
     const bool first_word = tb.first_word_sort && !multi;
     // keys: k1 (user order) -> key3, k2 (user order) -> key2; the sort key is k2
@@ -678,29 +692,60 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
     if (e != cudaSuccess) return e;
     if (first_word) {
         // Sort by k1 alone (8 passes). When every k1 differs, that is the order by
-        // (k1, k2); a tie anywhere sets the flag and the full sort below runs.
-        passes(tb.key_b, tb.key_a, tb.idx_a, tb.idx_b, 8, 18, 8, nullptr);  // result: key_b (k1 sorted), idx_a
-        k_word_ties<<<blocks_for(n, 256), 256, 0, st>>>(tb.key_b, n, ties);
-        k_full_sort_init<<<blocks_for(n, 256), 256, 0, st>>>(tb.key2, tb.key_a, tb.idx_a, n, ties);
-        L += 2;
+        // (k1, k2); a tie anywhere sets the flag, and the full sort runs after all.
+        passes(tb.key_b, tb.key_a, tb.idx_a, tb.idx_b, 8, 18, 8, nullptr, st);  // result: key_b (k1 sorted), idx_a
+        // Inside a stream capture the full sort becomes the body of a conditional
+        // graph node that runs only when the tie check sets its condition; launched
+        // directly, each of its kernels returns at once unless the flag is set.
+        cudaGraphConditionalHandle cond = 0;
+        cudaGraph_t cg = nullptr;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        const bool use_cond = tb.cond_stream && cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg) == cudaSuccess &&
+                              cs == cudaStreamCaptureStatusActive &&
+                              cudaGraphConditionalHandleCreate(&cond, cg, 0, cudaGraphCondAssignDefault) == cudaSuccess;
+        if (!use_cond) cudaGetLastError();
+        k_word_ties<<<blocks_for(n, 256), 256, 0, st>>>(tb.key_b, n, ties, cond, use_cond ? 1 : 0);
+        L += 1;
+        cudaStream_t fs = st;
+        if (use_cond) {
+            const cudaGraphNode_t *deps = nullptr;
+            size_t ndeps = 0;
+            if ((e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &ndeps)) != cudaSuccess) return e;
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = cond;
+            cp.conditional.type = cudaGraphCondTypeIf;
+            cp.conditional.size = 1;
+            cudaGraphNode_t node;
+            if ((e = cudaGraphAddNode(&node, cg, deps, ndeps, &cp)) != cudaSuccess) return e;
+            if ((e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
+                return e;
+            if ((e = cudaStreamBeginCaptureToGraph(tb.cond_stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                   cudaStreamCaptureModeRelaxed)) != cudaSuccess)
+                return e;
+            fs = tb.cond_stream;
+        }
+        k_full_sort_init<<<blocks_for(n, 256), 256, 0, fs>>>(tb.key2, tb.key_a, tb.idx_a, n, ties);
+        L += 1;
+        full_sort(fs, ties);
+        if (use_cond) {
+            cudaGraph_t body = nullptr;
+            if ((e = cudaStreamEndCapture(fs, &body)) != cudaSuccess) return e;
+        }
+    } else {
+        // LSD radix sort by (system, k1, k2): 8 passes on k2, 8 on k1 (then 2 on the system id)
+        full_sort(st, nullptr);
     }
-    // LSD radix sort by (system, k1, k2): 8 passes on k2, 8 on k1, 2 on the system id
-    // (after the first-word sort: only when it found ties).
-    const uint32_t *run_if = first_word ? ties : nullptr;
-    passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b, 0, 0, 8, run_if);    // result: key_a, idx_a
-    k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key3, tb.idx_a, tb.key_b, n, run_if);  // k1 in that order
-    passes(tb.key_b, tb.key_a, tb.idx_a, tb.idx_b, 8, 8, 8, run_if);    // result: key_b (k1 sorted), idx_a
-    L += 1;
     if (multi) {
         // then by system (16-bit ids, 2 stable passes; result back in key_a / idx_a)
         k_gather_sys<<<blocks_for(n, 256), 256, 0, st>>>(tb.sys_id, tb.idx_a, tb.key_a, nullptr, n);
-        passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b, 16, 16, 2, nullptr);
+        passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b, 16, 16, 2, nullptr, st);
         k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key3, tb.idx_a, tb.key_b, n, nullptr);  // k1 sorted
         k_gather_sys<<<blocks_for(n, 256), 256, 0, st>>>(tb.sys_id, tb.idx_a, nullptr, tb.sys_sorted, n);
         L += 3;
     } else if (!first_word) {
         // tell the host whether the next build may sort by the first word first
-        k_word_ties<<<blocks_for(n, 256), 256, 0, st>>>(tb.key_b, n, ties);
+        k_word_ties<<<blocks_for(n, 256), 256, 0, st>>>(tb.key_b, n, ties, 0, 0);
         L += 1;
     }
     k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key2, tb.idx_a, tb.key_a, n, nullptr);  // k2 sorted

@@ -16,6 +16,8 @@ struct TreeBuild {
     int first_word_sort;        // sort by the first key word (levels 1-21) first, and run the full
                                 // two-word sort only when that leaves ties (sc->word_ties); single
                                 // system only. The result is the same either way.
+    cudaStream_t cond_stream;   // captures the full sort into a conditional graph node (used only
+                                // while the build stream is being captured; null: never)
     int single;                 // the reference's FLOAT build: positions and masses are read as
                                 // floats; root cube, child centres, node masses and centres of
                                 // mass are computed in float arithmetic
