@@ -77,8 +77,12 @@ template <>
 struct WarpSmem<false> {
     GroupConsts gc;
     int2 stack[kStackCap];
-    float4 tc[32];            // (com - ref).xyz, -
-    float4 tq[32];            // q = (side/theta)^2, band half-width, reach mask bits, node ref bits
+    // The tile's mixed nodes, compacted and stored in pairs: pair j holds
+    // x0 x1 y0 y1 z0 z1 -q0 -q1 band0 band1 reach0 reach1 ref0 ref1 - - at 16 j
+    // ((com - ref).xyz, q = (side/theta)^2, the half-width of its error band, the
+    // mask of lanes that reached the node, the node). Once a pair is decided,
+    // its first two words hold the two open masks.
+    alignas(16) float mx[16 * 16];
     union {
         float4 lc[kListCap];  // adjoint: (com - ref).xyz, G m per entry
         float lp[4 * kListCap];  // forward: entries taken by some lanes, in pairs
@@ -96,6 +100,12 @@ struct WarpSmem<false> {
     uint32_t nm[kListCap];
     int nr[32];
 };
+
+// The paired lists and the mixed-node pairs are read with 16-byte loads.
+static_assert(offsetof(WarpSmem<false>, mx) % 16 == 0 && offsetof(WarpSmem<false>, lp) % 16 == 0 &&
+                  offsetof(WarpSmem<false>, lf) % 16 == 0 && offsetof(WarpSmem<false>, np) % 16 == 0 &&
+                  sizeof(WarpSmem<false>) % 16 == 0,
+              "16-byte shared loads need 16-byte aligned arrays");
 
 template <>
 struct WarpSmem<true> {
@@ -669,14 +679,11 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                 if constexpr (kFp64) {
                     s.tc[lane] = make_double4(cx, cy, cz, s.gc.S * so);
                     s.tr[lane] = make_int2((int)reach, ref);
-                } else {
-                    s.tc[lane] = make_float4(fcx, fcy, fcz, 0.f);
-                    s.tq[lane] = make_float4(qf, band, __uint_as_float(reach), __int_as_float(ref));
+                    __syncwarp();
                 }
-                __syncwarp();
-                uint32_t mm = intm;
                 if constexpr (kFp64) {
                     // the FP64 form decides every mixed node with the reference's own test
+                    uint32_t mm = intm;
                     while (mm) {
                         const int k = __ffs(mm) - 1;
                         mm &= mm - 1;
@@ -687,34 +694,56 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                         if (lane == k) my_open = om;
                     }
                 } else {
-                    // two mixed nodes per round: their tests are independent
+                    // The mixed nodes, compacted into pairs, are decided two per round
+                    // with packed FP32 arithmetic (the same roundings as the scalar
+                    // expressions: dx = c.x + (-px), r2 = fma(dz, dz, fma(dy, dy, dx dx)),
+                    // d = r2 + (-q)). Lane 0 stores each pair's open masks over the
+                    // pair's first two words; each mixed lane then reads its own.
+                    const int nmix = __popc(intm);
+                    const int mpos = __popc(intm & lt);
+                    if (mixed) {
+                        float *e = s.mx + 16 * (mpos >> 1) + (mpos & 1);
+                        e[0] = fcx; e[2] = fcy; e[4] = fcz; e[6] = -qf;
+                        e[8] = band; e[10] = __uint_as_float(reach); e[12] = __int_as_float(ref);
+                    }
+                    if (lane == 0 && (nmix & 1)) {
+                        // pad an odd count with an entry no lane reached
+                        float *e = s.mx + 16 * (nmix >> 1) + 1;
+                        e[0] = 0.f; e[2] = 0.f; e[4] = 0.f; e[6] = 0.f;
+                        e[8] = 0.f; e[10] = 0.f; e[12] = 0.f;
+                    }
+                    __syncwarp();
                     const float tiny_ = s.gc.tiny;
-                    while (mm) {
-                        const int k1 = __ffs(mm) - 1;
-                        mm &= mm - 1;
-                        const int k2 = mm ? __ffs(mm) - 1 : k1;
-                        if (mm) mm &= mm - 1;
-                        const float4 c1 = s.tc[k1], q1 = s.tq[k1];
-                        const float4 c2 = s.tc[k2], q2 = s.tq[k2];
-                        const uint32_t rk1 = __float_as_uint(q1.z), rk2 = __float_as_uint(q2.z);
-                        const float dx1 = c1.x - px, dy1 = c1.y - py, dz1 = c1.z - pz;
-                        const float dx2 = c2.x - px, dy2 = c2.y - py, dz2 = c2.z - pz;
-                        const float r21 = fmaf(dz1, dz1, fmaf(dy1, dy1, dx1 * dx1));
-                        const float r22 = fmaf(dz2, dz2, fmaf(dy2, dy2, dx2 * dx2));
-                        const float d1 = r21 - q1.x, d2 = r22 - q2.x;
+                    const uint64_t npx = f2pack(-px, -px), npy = f2pack(-py, -py), npz = f2pack(-pz, -pz);
+                    const uint32_t bit = 1u << lane;
+                    for (int k = 0; k < nmix; k += 2) {
+                        float *pr = s.mx + 8 * k;
+                        const float4 A = *reinterpret_cast<const float4 *>(pr);      // x0 x1 y0 y1
+                        const float4 B = *reinterpret_cast<const float4 *>(pr + 4);  // z0 z1 -q0 -q1
+                        const float4 C = *reinterpret_cast<const float4 *>(pr + 8);  // band0 band1 reach0 reach1
+                        const uint64_t dx = f2add(f2pack(A.x, A.y), npx);
+                        const uint64_t dy = f2add(f2pack(A.z, A.w), npy);
+                        const uint64_t dz = f2add(f2pack(B.x, B.y), npz);
+                        const uint64_t r2 = f2fma(dz, dz, f2fma(dy, dy, f2mul(dx, dx)));
+                        const uint64_t dd = f2add(r2, f2pack(B.z, B.w));
+                        float r21, r22, d1, d2;
+                        f2unpack(r2, r21, r22);
+                        f2unpack(dd, d1, d2);
+                        const uint32_t rk1 = __float_as_uint(C.z), rk2 = __float_as_uint(C.w);
                         bool open1 = d1 < 0.f, open2 = d2 < 0.f;
-                        const bool amb1 = ((rk1 >> lane) & 1u) && (fabsf(d1) <= q1.y || r21 <= tiny_);
-                        const bool amb2 = k2 != k1 && ((rk2 >> lane) & 1u) && (fabsf(d2) <= q2.y || r22 <= tiny_);
+                        const bool amb1 = (rk1 & bit) && (fabsf(d1) <= C.x || r21 <= tiny_);
+                        const bool amb2 = (rk2 & bit) && (fabsf(d2) <= C.y || r22 <= tiny_);
                         if (__any_sync(FULL, amb1 || amb2)) {
+                            const float2 R = *reinterpret_cast<const float2 *>(pr + 12);  // ref0 ref1
                             if (amb1) {
-                                const int node = __float_as_int(q1.w);
+                                const int node = __float_as_int(R.x);
                                 const double4 nd = t.onode[node];
                                 const double side = s.gc.S * exp2_neg(meta_level(t.ometa[node]));
                                 open1 = ref_open(single, nd.x, nd.y, nd.z, b.x, b.y, b.z, side, theta, theta_f);
                                 nfallback++;
                             }
                             if (amb2) {
-                                const int node = __float_as_int(q2.w);
+                                const int node = __float_as_int(R.y);
                                 const double4 nd = t.onode[node];
                                 const double side = s.gc.S * exp2_neg(meta_level(t.ometa[node]));
                                 open2 = ref_open(single, nd.x, nd.y, nd.z, b.x, b.y, b.z, side, theta, theta_f);
@@ -723,10 +752,13 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                         }
                         const uint32_t om1 = __ballot_sync(FULL, open1) & rk1;
                         const uint32_t om2 = __ballot_sync(FULL, open2) & rk2;
-                        if (lane == k1) my_open = om1;
-                        if (k2 != k1 && lane == k2) my_open = om2;
+                        // every lane has read the pair before the ballots complete
+                        if (lane == 0) *reinterpret_cast<uint2 *>(pr) = make_uint2(om1, om2);
                     }
+                    __syncwarp();
+                    if (mixed) my_open = __float_as_uint(s.mx[16 * (mpos >> 1) + (mpos & 1)]);
                 }
+                __syncwarp();
             }
 
             // ---- accepted bodies -> interaction list (compacted across lanes).
