@@ -103,10 +103,11 @@ struct nbody_ctx {
     double *sys_root = nullptr;
     int32_t *sys_root_node = nullptr;
     bool single_pass = false;  // nbody_barnes_hut: one system regardless of the layout
-    // The last tree build found no equal first key words, so the next one sorts by
-    // the first word first (TreeBuild::first_word_sort); the build checks this
-    // itself and falls back to the full sort on the device when it is wrong.
-    bool first_word_sort = false;
+    // Sort plan of the next tree build (TreeBuild::sort_p1, sort_p2): the full
+    // two-word sort until a build has measured its deepest split, then only the
+    // key bits that split needs plus one octree level. The build checks the plan
+    // itself and falls back to the full sort on the device when it is short.
+    int sort_p1 = 8, sort_p2 = 8;
     // CUDA graphs: one captured step replayed per step; per-offset graphs for the
     // adjoint's recompute and reverse steps. Rebuilt when their key changes.
     bool use_graphs = true;
@@ -221,6 +222,25 @@ int reserve(nbody_ctx *c, uint32_t n) {
     return NBODY_OK;
 }
 
+// The next build's sort plan from the last build's deepest split (the key bits
+// that separate every pair of neighbours) plus one octree level (3 bits), in
+// whole 8-bit passes: the top bits of the first word, or all of it and the top
+// bits of the second. A plan shrinks only by two passes or more, so that small
+// changes do not rebuild captured graphs; it grows at once after a build whose
+// plan was short (it ran the full sort then). No split measured: keep the plan.
+void next_sort_plan(nbody_ctx *c, uint32_t need_bits, bool short_plan) {
+    if (need_bits == 0) return;
+    const uint32_t bits = need_bits + 3;
+    int p1 = 8, p2 = 8;
+    if (bits <= 63) { p1 = (int)(bits + 7) / 8; p2 = 0; }
+    else if (bits <= 126) { p2 = (int)(bits - 63 + 7) / 8; }
+    const int cur = c->sort_p1 + c->sort_p2, want = p1 + p2;
+    if (short_plan || want > cur || cur - want >= 2) {
+        c->sort_p1 = p1;
+        c->sort_p2 = p2;
+    }
+}
+
 int check_status(nbody_ctx *c) {
     NB_CUDA(cudaStreamSynchronize(c->stream));
     const DevScalars &h = *c->hsc;
@@ -248,7 +268,9 @@ int check_status(nbody_ctx *c) {
     s.last_dt = h.dt_used;
     for (int k = 0; k < 3; k++) s.root_center[k] = h.root_center[k];
     s.root_side = h.root_side;
-    c->first_word_sort = h.word_ties == 0;
+    s.sort_passes = c->nsys > 1 ? 18u : (uint32_t)(c->sort_p1 + c->sort_p2) + (h.word_ties ? 16u : 0u);
+    s.sort_split_bits = h.max_prefix_bits;
+    next_sort_plan(c, h.max_prefix_bits, h.word_ties != 0);
     if (c->timing) {
         float ms[4] = {0, 0, 0, 0};
         for (int k = 0; k < 4; k++) cudaEventElapsedTime(&ms[k], c->ev[k], c->ev[k + 1]);
@@ -272,7 +294,9 @@ void tree_inputs(nbody_ctx *c, uint32_t n, bool want_vmax) {
     tb.vel_for_max = want_vmax ? c->vel : nullptr;
     tb.sc = c->sc;
     tb.single = single(c) ? 1 : 0;
-    tb.first_word_sort = c->first_word_sort ? 1 : 0;
+    tb.sort_p1 = c->sort_p1;
+    tb.sort_p2 = c->sort_p2;
+    tb.sort_checked = 1;
     tb.cond_stream = c->cond_stream;
 }
 
@@ -407,14 +431,14 @@ int download_acc(nbody_ctx *c, double *acc) {
 std::vector<unsigned char> graph_key(nbody_ctx *c, uint32_t extra) {
     struct K {
         uint32_t n, nsys, ngroups, extra;
-        int first_word;
+        int sort_p1, sort_p2;
         void *arena, *adj, *sys, *stream;
         nbody_params p;
         WalkLaunch wm, wf;
     } k;
     std::memset(&k, 0, sizeof k);
     k.n = c->n; k.nsys = c->nsys; k.ngroups = c->ngroups; k.extra = extra;
-    k.first_word = c->first_word_sort ? 1 : 0;
+    k.sort_p1 = c->sort_p1; k.sort_p2 = c->sort_p2;
     k.arena = c->arena; k.adj = c->adj_arena; k.sys = c->sys_arena; k.stream = (void *)c->stream;
     k.p = c->p; k.wm = c->wl_mixed; k.wf = c->wl_fp64;
     const unsigned char *b = (const unsigned char *)&k;

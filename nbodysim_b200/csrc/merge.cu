@@ -338,12 +338,14 @@ cudaError_t collide_fold(const MergeBufs &m, uint32_t k, const double *pos, cons
                          cudaStream_t st, unsigned *launches) {
     if (k == 0) return cudaSuccess;
     // stable LSD sort of the endpoints (ascending user index) by their 32-bit root
-    cudaError_t e = sort_prepare(m.skey_a, m.skey_a, nullptr, k, 16, m.sort_scratch, st, launches);
+    cudaError_t e = sort_reset(m.sort_scratch, k, st);
+    if (e == cudaSuccess)
+        e = sort_histograms(m.skey_a, 8, 0, nullptr, 0, 0, nullptr, 0, k, m.sort_scratch, nullptr, st, launches);
     if (e != cudaSuccess) return e;
     uint64_t *kin = m.skey_a, *kout = m.skey_b;
     uint32_t *iin = m.sidx_a, *iout = m.sidx_b;
     for (int q = 0; q < 4; q++) {
-        e = sort_pass(kin, iin, kout, iout, k, q, q, 8 * q, m.sort_scratch, &m.counters[kMcStatus], kMergeStatusSort,
+        e = sort_pass(kin, iin, kout, iout, k, q, digit_shift(8, q), m.sort_scratch, &m.counters[kMcStatus], kMergeStatusSort,
                       nullptr, st, launches);
         if (e != cudaSuccess) return e;
         uint64_t *tk = kin; kin = kout; kout = tk;

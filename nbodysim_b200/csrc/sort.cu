@@ -22,36 +22,48 @@ constexpr uint32_t kTile = kThreads * kItems;
 constexpr uint32_t kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kValue = (1u << 30) - 1;
 constexpr uint32_t kSpinLimit = 1u << 20;
 
-// Global digit histograms of every pass. Pass p sorts by byte (p % 8) of word
-// p / 8, where the words are, in order, `w0` (8 passes), `w1` (8 passes) and
-// the 16-bit `w2` (2 passes, optional).
-__global__ void k_hist_all(const uint64_t *__restrict__ w0, const uint64_t *__restrict__ w1,
-                           const uint32_t *__restrict__ w2, uint32_t n, int npass, uint32_t *__restrict__ ghist) {
+// Global digit histograms: pa passes of wa (slots slot_a..), pb of wb (slot_b..)
+// and, with wc non-null, the two bytes of wc (slot_c, slot_c + 1). Shared
+// counters are indexed by the pass's position in that list.
+__global__ void k_hist(const uint64_t *__restrict__ wa, int pa, int slot_a, const uint64_t *__restrict__ wb, int pb,
+                       int slot_b, const uint32_t *__restrict__ wc, int slot_c, uint32_t n,
+                       uint32_t *__restrict__ ghist, const uint32_t *run_if) {
     __shared__ uint32_t s_h[18 * 256];
-    for (int i = threadIdx.x; i < npass * 256; i += blockDim.x) s_h[i] = 0;
+    if (run_if && *run_if == 0u) return;
+    const int pc = wc ? 2 : 0, np = pa + pb + pc;
+    for (int i = threadIdx.x; i < np * 256; i += blockDim.x) s_h[i] = 0;
     __syncthreads();
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint64_t a = w0[i], b = w1[i];
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            atomicAdd(&s_h[k * 256 + ((a >> (8 * k)) & 255u)], 1u);
-            atomicAdd(&s_h[(8 + k) * 256 + ((b >> (8 * k)) & 255u)], 1u);
+        if (pa > 0) {
+            const uint64_t a = wa[i];
+            for (int k = 0; k < pa; k++) atomicAdd(&s_h[k * 256 + ((a >> digit_shift(pa, k)) & 255u)], 1u);
         }
-        if (npass > 16) {
-            const uint32_t c = w2[i];
-            atomicAdd(&s_h[16 * 256 + (c & 255u)], 1u);
-            atomicAdd(&s_h[17 * 256 + ((c >> 8) & 255u)], 1u);
+        if (pb > 0) {
+            const uint64_t b = wb[i];
+            for (int k = 0; k < pb; k++) atomicAdd(&s_h[(pa + k) * 256 + ((b >> digit_shift(pb, k)) & 255u)], 1u);
+        }
+        if (pc) {
+            const uint32_t c = wc[i];
+            atomicAdd(&s_h[(pa + pb) * 256 + (c & 255u)], 1u);
+            atomicAdd(&s_h[(pa + pb + 1) * 256 + ((c >> 8) & 255u)], 1u);
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < npass * 256; i += blockDim.x)
-        if (s_h[i]) atomicAdd(&ghist[i], s_h[i]);
+    for (int i = threadIdx.x; i < np * 256; i += blockDim.x) {
+        const int k = i >> 8;
+        const int slot = k < pa ? slot_a + k : k < pa + pb ? slot_b + (k - pa) : slot_c + (k - pa - pb);
+        if (s_h[i]) atomicAdd(&ghist[slot * 256 + (i & 255)], s_h[i]);
+    }
 }
 
-// Exclusive scan of each pass's 256 counts (one block per pass).
-__global__ void k_hist_scan(uint32_t *__restrict__ ghist) {
+// Exclusive scan of each pass's 256 counts (one block per pass, in the order of k_hist).
+__global__ void k_hist_scan(uint32_t *__restrict__ ghist, int pa, int slot_a, int pb, int slot_b, int slot_c,
+                            const uint32_t *run_if) {
     __shared__ uint32_t s[256];
-    uint32_t *h = ghist + 256 * blockIdx.x;
+    if (run_if && *run_if == 0u) return;
+    const int k = blockIdx.x;
+    const int slot = k < pa ? slot_a + k : k < pa + pb ? slot_b + (k - pa) : slot_c + (k - pa - pb);
+    uint32_t *h = ghist + 256 * slot;
     const int t = threadIdx.x;
     const uint32_t x = h[t];
     s[t] = x;
@@ -206,34 +218,38 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint64_t *__restric
 
 }  // namespace
 
-// Scratch: the digit offsets of up to 18 passes (histogram slots), then the
-// tile status words and the ticket of up to kPassSlots passes.
-constexpr int kHistSlots = 18;
-constexpr int kPassSlots = 26;
-
+// Scratch: the digit offsets of every slot, then the tile status words of
+// every slot, then one ticket per slot.
 size_t sort_scratch_bytes(uint32_t n) {
     const size_t tiles = (n + kTile - 1) / kTile;
-    return 4 * (kHistSlots * 256 + kPassSlots * tiles * 256 + 32);
+    return 4 * (kSortSlots * 256 + kSortSlots * tiles * 256 + 64);
 }
 
-cudaError_t sort_prepare(const uint64_t *w0, const uint64_t *w1, const uint32_t *w2, uint32_t n, int npass,
-                         uint32_t *scratch, cudaStream_t st, unsigned *launches) {
-    cudaError_t e = cudaMemsetAsync(scratch, 0, sort_scratch_bytes(n), st);
-    if (e != cudaSuccess) return e;
+cudaError_t sort_reset(uint32_t *scratch, uint32_t n, cudaStream_t st) {
+    return cudaMemsetAsync(scratch, 0, sort_scratch_bytes(n), st);
+}
+
+cudaError_t sort_histograms(const uint64_t *wa, int pa, int slot_a, const uint64_t *wb, int pb, int slot_b,
+                            const uint32_t *wc, int slot_c, uint32_t n, uint32_t *scratch, const uint32_t *run_if,
+                            cudaStream_t st, unsigned *launches) {
+    if (!wa) pa = 0;
+    if (!wb) pb = 0;
+    const int np = pa + pb + (wc ? 2 : 0);
+    if (np == 0) return cudaSuccess;
     const unsigned blocks = (unsigned)std::min<size_t>(1184, (n + 255) / 256);
-    k_hist_all<<<blocks ? blocks : 1, 256, 0, st>>>(w0, w1, w2, n, npass, scratch);
-    k_hist_scan<<<npass, 256, 0, st>>>(scratch);
+    k_hist<<<blocks ? blocks : 1, 256, 0, st>>>(wa, pa, slot_a, wb, pb, slot_b, wc, slot_c, n, scratch, run_if);
+    k_hist_scan<<<np, 256, 0, st>>>(scratch, pa, slot_a, pb, slot_b, slot_c, run_if);
     *launches += 2;
     return cudaGetLastError();
 }
 
-cudaError_t sort_pass(const uint64_t *kin, const uint32_t *iin, uint64_t *kout, uint32_t *iout, uint32_t n, int pass,
-                      int slot, int shift, uint32_t *scratch, uint32_t *err, uint32_t err_bit, const uint32_t *run_if,
+cudaError_t sort_pass(const uint64_t *kin, const uint32_t *iin, uint64_t *kout, uint32_t *iout, uint32_t n, int slot,
+                      int shift, uint32_t *scratch, uint32_t *err, uint32_t err_bit, const uint32_t *run_if,
                       cudaStream_t st, unsigned *launches) {
     const size_t tiles = (n + kTile - 1) / kTile;
-    uint32_t *goff = scratch + 256 * pass;
-    uint32_t *status = scratch + kHistSlots * 256 + (size_t)slot * tiles * 256;
-    uint32_t *ticket = scratch + kHistSlots * 256 + kPassSlots * tiles * 256 + slot;
+    uint32_t *goff = scratch + 256 * slot;
+    uint32_t *status = scratch + kSortSlots * 256 + (size_t)slot * tiles * 256;
+    uint32_t *ticket = scratch + kSortSlots * 256 + kSortSlots * tiles * 256 + slot;
     k_onesweep<<<(unsigned)tiles, kThreads, 0, st>>>(kin, iin, kout, iout, n, shift, goff, status, ticket, err,
                                                      err_bit, run_if);
     *launches += 1;

@@ -180,11 +180,13 @@ __device__ inline void descend_words(const double *p, const double *root, int wo
     for (int w = 0; w < words; w++) out[w] = descend_word<T>(x, y, z, cx, cy, cz, s);
 }
 
-// Two key words per particle: levels 1..21 (k1) and 22..42 (k2). Escaped
+// Key words per particle: levels 1..21 (k1) and 22..42 (k2). Escaped
 // particles can make the root cube many orders of magnitude larger than the
-// bulk of the system, so the first 21 levels alone do not separate it.
+// bulk of the system, so the first 21 levels alone do not separate it. With
+// k2_user null only k1 is computed (a sort plan that needs no second word).
+// The sort key (k1 or k2) goes to `sortkey`, the identity to `idx`.
 __global__ void k_keys(const double *__restrict__ pos, uint32_t n, const DevScalars *sc,
-                       uint64_t *__restrict__ k1_user, uint64_t *__restrict__ k2_sortkey,
+                       uint64_t *__restrict__ k1_user, uint64_t *__restrict__ sortkey,
                        uint64_t *__restrict__ k2_user, uint32_t *__restrict__ idx,
                        const uint32_t *__restrict__ sys_id, const double *__restrict__ sys_root, int single,
                        int sort_by_k1) {
@@ -199,13 +201,29 @@ __global__ void k_keys(const double *__restrict__ pos, uint32_t n, const DevScal
         root[3] = sc->root_side;
     }
     const double p[3] = {pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2]};
+    const int words = k2_user ? 2 : 1;
+    uint64_t w[2] = {0, 0};
+    if (single) descend_words<float>(p, root, words, w);
+    else descend_words<double>(p, root, words, w);
+    k1_user[i] = w[0];
+    sortkey[i] = sort_by_k1 ? w[0] : w[1];
+    if (k2_user) k2_user[i] = w[1];
+    idx[i] = i;
+}
+
+// The second key words (single system), for a full sort that follows a plan
+// without them; nothing unless *run_if is non-zero.
+__global__ void k_keys_second(const double *__restrict__ pos, uint32_t n, const DevScalars *sc,
+                              uint64_t *__restrict__ k2_user, int single, const uint32_t *run_if) {
+    if (*run_if == 0u) return;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double root[4] = {sc->root_center[0], sc->root_center[1], sc->root_center[2], sc->root_side};
+    const double p[3] = {pos[3 * (size_t)i], pos[3 * (size_t)i + 1], pos[3 * (size_t)i + 2]};
     uint64_t w[2];
     if (single) descend_words<float>(p, root, 2, w);
     else descend_words<double>(p, root, 2, w);
-    k1_user[i] = w[0];
-    k2_sortkey[i] = sort_by_k1 ? w[0] : w[1];
     k2_user[i] = w[1];
-    idx[i] = i;
 }
 
 // dst[j] = src[idx[j]]; with run_if non-null, only when *run_if is non-zero.
@@ -216,14 +234,16 @@ __global__ void k_gather_key(const uint64_t *__restrict__ src, const uint32_t *_
     if (j < n) dst[j] = src[idx[j]];
 }
 
-// Flags equal neighbours among the sorted first key words: then the first 21
-// octree levels do not separate every particle and the second word is needed.
-// Inside a captured graph (use_cond) it also sets the condition of the graph
-// node that holds the full sort.
-__global__ void k_word_ties(const uint64_t *__restrict__ k1_sorted, uint32_t n, uint32_t *ties,
-                            cudaGraphConditionalHandle cond, int use_cond) {
+// Flags equal neighbours over the bits a sort plan covered: (k1 >> s1), and
+// with k2 non-null also (k2 >> s2). Then the plan did not separate every
+// particle and the full sort is needed. Inside a captured graph (use_cond) it
+// also sets the condition of the graph node that holds the full sort.
+__global__ void k_prefix_ties(const uint64_t *__restrict__ k1_sorted, const uint64_t *__restrict__ k2_sorted,
+                              int s1, int s2, uint32_t n, uint32_t *ties, cudaGraphConditionalHandle cond,
+                              int use_cond) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool tie = j + 1 < n && k1_sorted[j] == k1_sorted[j + 1];
+    bool tie = j + 1 < n && (k1_sorted[j] >> s1) == (k1_sorted[j + 1] >> s1);
+    if (tie && k2_sorted) tie = (k2_sorted[j] >> s2) == (k2_sorted[j + 1] >> s2);
     if (__any_sync(0xffffffffu, tie) && (threadIdx.x & 31) == 0) {
         atomicOr(ties, 1u);
         if (use_cond) cudaGraphSetConditional(cond, 1u);
@@ -428,9 +448,13 @@ __device__ inline int level_of(int delta) { return min(delta / 3, kMaxLevels); }
 
 __global__ void k_radix_tree(KeyView kv, int32_t *__restrict__ bleft, int32_t *__restrict__ bright,
                              int32_t *__restrict__ bparent, int32_t *__restrict__ leaf_bparent,
-                             int32_t *__restrict__ bdelta) {
+                             int32_t *__restrict__ bdelta, uint32_t *max_prefix_bits) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = kv.n;
+    // the deepest split: key bits that separate every pair of neighbours
+    const int dn = i < n - 1 ? kv.delta(i, i + 1) : -1;
+    const int wmax = __reduce_max_sync(0xffffffffu, dn);
+    if ((threadIdx.x & 31) == 0 && wmax >= 0) atomicMax(max_prefix_bits, (uint32_t)wmax + 1u);
     if (i >= n - 1) return;
     // With several systems, the internal nodes of the system [s, e) are s..e-2:
     // the last particle of a system indexes no internal node.
@@ -659,44 +683,63 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
     }
     uint32_t *sort_err = &tb.sc->status;
     uint32_t *ties = &tb.sc->word_ties;
-    // one LSD pass sequence: count passes ping-ponging kin/kout and iin/iout (an
-    // even count leaves the result in kin/iin), histogram passes from `first`,
-    // status slots from `slot`
-    auto passes = [&](uint64_t *kin, uint64_t *kout, uint32_t *iin, uint32_t *iout, int first, int slot, int count,
+    // `count` LSD passes with the digits of a `plan`-pass sort of one word
+    // (digit_shift), histogram and status slots from `slot`, ping-ponging
+    // (kin, iin) and (kout, iout): an even count leaves the result in (kin, iin),
+    // an odd one in (kout, iout).
+    auto passes = [&](uint64_t *kin, uint64_t *kout, uint32_t *iin, uint32_t *iout, int count, int plan, int slot,
                       const uint32_t *run_if, cudaStream_t s) {
         for (int q = 0; q < count; q++) {
-            sort_pass(kin, iin, kout, iout, n, first + q, slot + q, 8 * q, tb.sort_scratch, sort_err, kStatusSortStall,
-                      run_if, s, &L);
+            sort_pass(kin, iin, kout, iout, n, slot + q, digit_shift(plan, q), tb.sort_scratch, sort_err,
+                      kStatusSortStall, run_if, s, &L);
             uint64_t *tk = kin; kin = kout; kout = tk;
             uint32_t *ti = iin; iin = iout; iout = ti;
         }
     };
-    // the LSD sort by (k1, k2) on stream `s`: 8 passes on k2, the gather of k1, 8
-    // passes on k1 (result: key_b sorted by k1, idx_a)
-    auto full_sort = [&](cudaStream_t s, const uint32_t *run_if) {
-        passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b, 0, 0, 8, run_if, s);    // result: key_a, idx_a
-        k_gather_key<<<blocks_for(n, 256), 256, 0, s>>>(tb.key3, tb.idx_a, tb.key_b, n, run_if);  // k1 in that order
-        passes(tb.key_b, tb.key_a, tb.idx_a, tb.idx_b, 8, 8, 8, run_if, s);    // result: key_b (k1 sorted), idx_a
+    auto gather = [&](const uint64_t *src, uint64_t *dst, const uint32_t *run_if, cudaStream_t s) {
+        k_gather_key<<<blocks_for(n, 256), 256, 0, s>>>(src, tb.idx_a, dst, n, run_if);
         L += 1;
     };
-    const bool first_word = tb.first_word_sort && !multi;
-    // keys: k1 (user order) -> key3, k2 (user order) -> key2; the sort key is k2
-    // (key_a) or, sorting by the first word first, k1 (key_b)
-    k_keys<<<blocks_for(n, 256), 256, 0, st>>>(tb.pos, n, tb.sc, tb.key3, first_word ? tb.key_b : tb.key_a, tb.key2,
-                                               tb.idx_a, multi ? tb.sys_id : nullptr, tb.sys_root, tb.single,
-                                               first_word ? 1 : 0);
-    L += 2;
-    // Histograms: passes 0-7 by the bytes of k2, 8-15 of k1, 16-17 of the system id.
-    cudaError_t e = sort_prepare(tb.key2, tb.key3, multi ? tb.sys_id : nullptr, n, multi ? 18 : 16, tb.sort_scratch,
-                                 st, &L);
-    if (e != cudaSuccess) return e;
-    if (first_word) {
-        // Sort by k1 alone (8 passes). When every k1 differs, that is the order by
-        // (k1, k2); a tie anywhere sets the flag, and the full sort runs after all.
-        passes(tb.key_b, tb.key_a, tb.idx_a, tb.idx_b, 8, 18, 8, nullptr, st);  // result: key_b (k1 sorted), idx_a
-        // Inside a stream capture the full sort becomes the body of a conditional
-        // graph node that runs only when the tie check sets its condition; launched
-        // directly, each of its kernels returns at once unless the flag is set.
+    // Slots: passes on k2 0-7, on k1 8-15, on the system id 16-17; the full sort
+    // after a plan that left ties, k2 18-25 and k1 26-33.
+    // Every plan leaves k1 in sorted order in key_b and the permutation in idx_a
+    // (a plan with an odd pass count starts in the other buffers). The user-order
+    // words: k1 in key3, k2 in key2.
+    const int p2 = multi ? 8 : tb.sort_p2, p1 = multi ? 8 : tb.sort_p1;
+    const bool checked = !multi && tb.sort_checked && !(p2 >= 8 && p1 >= 8);
+    if (p2 > 0) {
+        uint64_t *k0 = (p2 & 1) ? tb.key_b : tb.key_a, *k0o = (p2 & 1) ? tb.key_a : tb.key_b;
+        uint32_t *i0 = (p2 & 1) ? tb.idx_b : tb.idx_a, *i0o = (p2 & 1) ? tb.idx_a : tb.idx_b;
+        k_keys<<<blocks_for(n, 256), 256, 0, st>>>(tb.pos, n, tb.sc, tb.key3, k0, tb.key2, i0,
+                                                   multi ? tb.sys_id : nullptr, tb.sys_root, tb.single, 0);
+        L += 1;
+        cudaError_t e = sort_reset(tb.sort_scratch, n, st);
+        if (e == cudaSuccess)
+            e = sort_histograms(tb.key2, p2, 0, tb.key3, 8, 8, multi ? tb.sys_id : nullptr, 16, n, tb.sort_scratch,
+                                nullptr, st, &L);
+        if (e != cudaSuccess) return e;
+        passes(k0, k0o, i0, i0o, p2, p2, 0, nullptr, st);                   // result: key_a, idx_a
+        gather(tb.key3, tb.key_b, nullptr, st);                               // k1 in that order
+        passes(tb.key_b, tb.key_a, tb.idx_a, tb.idx_b, 8, 8, 8, nullptr, st);  // result: key_b, idx_a
+    } else {
+        uint64_t *k0 = (p1 & 1) ? tb.key_a : tb.key_b, *k0o = (p1 & 1) ? tb.key_b : tb.key_a;
+        uint32_t *i0 = (p1 & 1) ? tb.idx_b : tb.idx_a, *i0o = (p1 & 1) ? tb.idx_a : tb.idx_b;
+        k_keys<<<blocks_for(n, 256), 256, 0, st>>>(tb.pos, n, tb.sc, tb.key3, k0, nullptr, i0, nullptr, tb.sys_root,
+                                                   tb.single, 1);
+        L += 1;
+        cudaError_t e = sort_reset(tb.sort_scratch, n, st);
+        if (e == cudaSuccess)
+            e = sort_histograms(tb.key3, p1, 8, nullptr, 0, 0, nullptr, 0, n, tb.sort_scratch, nullptr, st, &L);
+        if (e != cudaSuccess) return e;
+        passes(k0, k0o, i0, i0o, p1, p1, 8, nullptr, st);  // result: key_b, idx_a
+    }
+    if (checked) {
+        // Equal neighbours over the bits the plan sorted mean it did not separate
+        // every particle: then the full sort runs. Inside a stream capture it is
+        // the body of a conditional graph node that runs only when the check sets
+        // its condition; launched directly, each of its kernels returns at once
+        // unless the flag is set.
+        if (p2 > 0) gather(tb.key2, tb.key_a, nullptr, st);  // k2 in sorted order, for the check
         cudaGraphConditionalHandle cond = 0;
         cudaGraph_t cg = nullptr;
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -704,9 +747,12 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
                               cs == cudaStreamCaptureStatusActive &&
                               cudaGraphConditionalHandleCreate(&cond, cg, 0, cudaGraphCondAssignDefault) == cudaSuccess;
         if (!use_cond) cudaGetLastError();
-        k_word_ties<<<blocks_for(n, 256), 256, 0, st>>>(tb.key_b, n, ties, cond, use_cond ? 1 : 0);
+        k_prefix_ties<<<blocks_for(n, 256), 256, 0, st>>>(tb.key_b, p2 > 0 ? tb.key_a : nullptr,
+                                                          p2 > 0 ? 0 : digit_shift(p1, 0), p2 > 0 ? digit_shift(p2, 0) : 0,
+                                                          n, ties, cond, use_cond ? 1 : 0);
         L += 1;
         cudaStream_t fs = st;
+        cudaError_t e;
         if (use_cond) {
             const cudaGraphNode_t *deps = nullptr;
             size_t ndeps = 0;
@@ -725,33 +771,39 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
                 return e;
             fs = tb.cond_stream;
         }
+        // the full sort by (k1, k2): 8 passes on k2, the gather of k1, 8 passes on k1
+        if (p2 == 0) {
+            k_keys_second<<<blocks_for(n, 256), 256, 0, fs>>>(tb.pos, n, tb.sc, tb.key2, tb.single, ties);
+            L += 1;
+        }
+        if ((e = sort_histograms(tb.key2, 8, 18, tb.key3, 8, 26, nullptr, 0, n, tb.sort_scratch, ties, fs, &L)) !=
+            cudaSuccess)
+            return e;
         k_full_sort_init<<<blocks_for(n, 256), 256, 0, fs>>>(tb.key2, tb.key_a, tb.idx_a, n, ties);
         L += 1;
-        full_sort(fs, ties);
+        passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b, 8, 8, 18, ties, fs);  // result: key_a, idx_a
+        gather(tb.key3, tb.key_b, ties, fs);
+        passes(tb.key_b, tb.key_a, tb.idx_a, tb.idx_b, 8, 8, 26, ties, fs);  // result: key_b, idx_a
+        gather(tb.key2, tb.key_a, ties, fs);                                  // k2 sorted
         if (use_cond) {
             cudaGraph_t body = nullptr;
             if ((e = cudaStreamEndCapture(fs, &body)) != cudaSuccess) return e;
         }
-    } else {
-        // LSD radix sort by (system, k1, k2): 8 passes on k2, 8 on k1 (then 2 on the system id)
-        full_sort(st, nullptr);
     }
     if (multi) {
         // then by system (16-bit ids, 2 stable passes; result back in key_a / idx_a)
         k_gather_sys<<<blocks_for(n, 256), 256, 0, st>>>(tb.sys_id, tb.idx_a, tb.key_a, nullptr, n);
-        passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b, 16, 16, 2, nullptr, st);
-        k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key3, tb.idx_a, tb.key_b, n, nullptr);  // k1 sorted
+        passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b, 2, 8, 16, nullptr, st);
+        gather(tb.key3, tb.key_b, nullptr, st);  // k1 sorted
         k_gather_sys<<<blocks_for(n, 256), 256, 0, st>>>(tb.sys_id, tb.idx_a, nullptr, tb.sys_sorted, n);
-        L += 3;
-    } else if (!first_word) {
-        // tell the host whether the next build may sort by the first word first
-        k_word_ties<<<blocks_for(n, 256), 256, 0, st>>>(tb.key_b, n, ties, 0, 0);
-        L += 1;
+        L += 2;
     }
-    k_gather_key<<<blocks_for(n, 256), 256, 0, st>>>(tb.key2, tb.idx_a, tb.key_a, n, nullptr);  // k2 sorted
+    // k2 sorted into key_a (a checked plan has it already, or needs none: with
+    // every k1 prefix distinct, nothing reads k2)
+    if (!checked) gather(tb.key2, tb.key_a, nullptr, st);
     if (tb.mass_ready && !multi) cudaStreamWaitEvent(st, tb.mass_ready, 0);  // the first reader of the masses
     k_gather_bodies<<<blocks_for(n, 256), 256, 0, st>>>(tb.idx_a, tb.pos, tb.mass, tb.body, n, tb.sc, tb.single);
-    L += 2;
+    L += 1;
     *launches += L;
     if (n < 2) return cudaGetLastError();
     L = 0;
@@ -761,7 +813,7 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
     KeyView kv{tb.key_b, tb.key_a, tb.key3, (int)n, sys_sorted};
     const uint32_t m = n - 1;
     k_radix_tree<<<blocks_for(m, 256), 256, 0, st>>>(kv, tb.bleft, tb.bright, tb.bparent, tb.leaf_bparent,
-                                                      tb.bdelta);
+                                                      tb.bdelta, &tb.sc->max_prefix_bits);
     k_head_flags<<<blocks_for(m, 256), 256, 0, st>>>(tb.bparent, tb.bdelta, m, tb.head_flag);
     cudaMemcpyAsync(tb.head_id, tb.head_flag, sizeof(uint32_t) * m, cudaMemcpyDeviceToDevice, st);
     L += 3 + scan_exclusive(tb.head_id, m, tb.scan_tmp, &tb.sc->n_onodes, st);

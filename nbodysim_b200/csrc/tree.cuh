@@ -13,9 +13,14 @@ struct TreeBuild {
                                 // the build waits for this event before it first reads them
     const double *vel_for_max;  // non-null: also reduce max |v| (adaptive dt)
     int keep_root;              // rebuild inside the root cube already in sc (single system)
-    int first_word_sort;        // sort by the first key word (levels 1-21) first, and run the full
-                                // two-word sort only when that leaves ties (sc->word_ties); single
-                                // system only. The result is the same either way.
+    // Sort plan (single system). sort_p2 passes sort the top 8 sort_p2 bits of
+    // the second key word (levels 22-42; 0: none), then sort_p1 passes the top
+    // 8 sort_p1 bits of the first word (levels 1-21); 8 passes take a whole
+    // word. With sort_checked, a check for equal neighbours over those bits
+    // follows and the full two-word sort runs on the device only when it finds
+    // one (sc->word_ties), so a plan that covers too few bits costs time, not
+    // results. Several systems always take the full sort.
+    int sort_p1, sort_p2, sort_checked;
     cudaStream_t cond_stream;   // captures the full sort into a conditional graph node (used only
                                 // while the build stream is being captured; null: never)
     int single;                 // the reference's FLOAT build: positions and masses are read as

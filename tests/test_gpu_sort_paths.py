@@ -1,9 +1,12 @@
-"""GPU: the two ways the octree build sorts its keys give the same octree.
+"""GPU: every sort plan of the octree build gives the same octree.
 
-A build sorts by the first key word (octree levels 1-21) alone when the last
-build found no two particles sharing it, and falls back on the device to the
-full two-word sort when the new state has such ties. Whatever the prediction,
-accepted-node counts must equal the oracle's and the forces must not change."""
+A fresh context sorts both key words in full (16 passes of 8 bits). Later builds
+sort only the key bits that the last build's deepest split needed plus one octree
+level: the top bits of the first word (octree levels 1-21), or all of it and the
+top bits of the second (levels 22-42). A check for equal neighbours over those
+bits follows every planned sort, and the full sort runs on the device when the
+plan was short. Whatever the plan, accepted-node counts must equal the oracle's
+and the forces must not change."""
 import numpy as np
 import pytest
 
@@ -19,33 +22,83 @@ def clustered_with_outliers(nb, n=5000):
     return pos, mass
 
 
+def planned_passes(split_bits):
+    """Passes of the plan that covers `split_bits` plus one octree level."""
+    bits = split_bits + 3
+    if bits <= 63:
+        return (bits + 7) // 8
+    return 8 + (bits - 63 + 7) // 8 if bits <= 126 else 16
+
+
 @pytest.mark.parametrize("precision", [0, 1])
-def test_first_word_sort_and_fallback_agree(nb, orc, precision):
-    spread, _, ms = nb.generate(20000, gen_type=2, size=1024.0, seed=5)  # no shared first words
+def test_sort_plans_agree(nb, orc, precision):
+    spread, _, ms = nb.generate(20000, gen_type=2, size=1024.0, seed=5)
     tied, mt = clustered_with_outliers(nb)
     _, rc_tied = orc.forces(tied, mt, 0.5)
     _, rc_spread = orc.forces(spread, ms, 0.5)
     with nb.Engine(precision=precision) as fresh:
         a_tied_full, c_tied_full = fresh.barnes_hut(tied, mt, counts=True)  # a fresh context sorts both words
+        st = fresh.stats()
+        assert st["sort_passes"] == 16 and st["sort_split_bits"] > 63
     assert np.array_equal(c_tied_full, rc_tied)
     with nb.Engine(precision=precision) as e:
-        for _ in range(2):  # the second call sorts by the first word only
-            a_s, c_s = e.barnes_hut(spread, ms, counts=True)
-            assert np.array_equal(c_s, rc_spread)
-        # predicted "no ties", but this state has them: the device falls back to the full sort
+        a_s, c_s = e.barnes_hut(spread, ms, counts=True)
+        assert np.array_equal(c_s, rc_spread)
+        st = e.stats()
+        assert st["sort_passes"] == 16
+        split = st["sort_split_bits"]
+        assert 3 <= split <= 63 - 3
+        # the second call sorts only the top bits of the first word
+        a_s1, c_s1 = e.barnes_hut(spread, ms, counts=True)
+        assert e.stats()["sort_passes"] == planned_passes(split) < 8
+        assert np.array_equal(c_s1, rc_spread) and np.array_equal(a_s1, a_s)
+        # planned for the spread state, but this one needs the second word: the
+        # device runs the full sort after the planned one
         a_t, c_t = e.barnes_hut(tied, mt, counts=True)
+        st = e.stats()
+        assert st["sort_passes"] == planned_passes(split) + 16
         assert np.array_equal(c_t, rc_tied)
         assert np.array_equal(a_t, a_tied_full)
-        # and now the full sort is predicted; back to the spread state (no ties) once more
-        a_t2, _ = e.barnes_hut(tied, mt, counts=True)
-        assert np.array_equal(a_t2, a_tied_full)
+        # now all of the first word and the top bits of the second
+        split_t = st["sort_split_bits"]
+        a_t2, c_t2 = e.barnes_hut(tied, mt, counts=True)
+        assert 8 < e.stats()["sort_passes"] == planned_passes(split_t) < 16
+        assert np.array_equal(c_t2, rc_tied) and np.array_equal(a_t2, a_tied_full)
+        # back to the spread state: the larger plan covers it, then the plan shrinks
         a_s2, c_s2 = e.barnes_hut(spread, ms, counts=True)
+        assert e.stats()["sort_passes"] == planned_passes(split_t)
         assert np.array_equal(c_s2, rc_spread) and np.array_equal(a_s2, a_s)
+        a_s3, _ = e.barnes_hut(spread, ms, counts=True)
+        assert e.stats()["sort_passes"] == planned_passes(split)
+        assert np.array_equal(a_s3, a_s)
 
 
-def test_graph_replay_across_the_switch(nb):
+@pytest.mark.parametrize("single", [False, True])
+def test_plan_one_level_short(nb, orc, single):
+    """A state whose deepest split lies below the plan's extra level: the check
+    finds the equal neighbours and the full sort runs (FP64 and FLOAT builds)."""
+    pos, _, mass = nb.generate(20000, gen_type=2, size=1024.0, seed=7)
+    deeper = pos.copy()
+    deeper[1] = deeper[0] + np.array([1e-4, -2e-4, 1e-4])  # a pair much closer than any other
+    dt = 4 if single else 8
+    _, rc = orc.forces(deeper, mass, 0.5, single=single)
+    with nb.Engine(datatype_bytes=dt) as e:
+        e.barnes_hut(pos, mass)
+        e.barnes_hut(pos, mass)
+        split = e.stats()["sort_split_bits"]
+        acc, cnt = e.barnes_hut(deeper, mass, counts=True)
+        st = e.stats()
+        assert st["sort_split_bits"] > split + 3
+        assert st["sort_passes"] == planned_passes(split) + 16
+        assert np.array_equal(cnt, rc)
+    with nb.Engine(datatype_bytes=dt) as fresh:
+        acc_full, cnt_full = fresh.barnes_hut(deeper, mass, counts=True)
+    assert np.array_equal(acc, acc_full) and np.array_equal(cnt, cnt_full)
+
+
+def test_graph_replay_across_plans(nb):
     """Steps replayed from captured graphs keep their results when the state
-    moves between the two sort paths (each path is its own captured graph)."""
+    moves between sort plans (each plan is its own captured graph)."""
     spread, vel, ms = nb.generate(20000, gen_type=2, size=1024.0, seed=5)
     out = []
     for graphs in (True, False):
@@ -56,5 +109,7 @@ def test_graph_replay_across_the_switch(nb):
             tied, mt = clustered_with_outliers(nb)
             e.set_particles(tied, np.zeros_like(tied), mt)
             e.step(2)
+            e.set_particles(spread, vel, ms)
+            e.step(3)
             out.append(e.get_particles())
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
