@@ -288,6 +288,7 @@ def run_ours(args) -> None:
         ph["walk"].append(s_["ms_walk"]); ph["update"].append(s_["ms_update"])
         ph["inter"].append(s_["interactions"])
     eng.set_timing(False)
+    sort_plan = {"passes": s_["sort_passes"], "split_bits": s_["sort_split_bits"]}
     walk_ms = float(np.mean(ph["walk"]))
     walk_inter = float(np.mean(ph["inter"]))
 
@@ -430,6 +431,7 @@ def run_ours(args) -> None:
     details = {"phases_ms": {k: float(np.mean(v)) for k, v in ph.items() if k != "inter"},
                "fp64_form_walk_ms": fp64_walk_ms, "vs_fp64_direct_sum": direct, "adjoint": adjoint,
                "ensemble": ensemble, "configs": configs, "evolved": evolved, "walk_shape": walk_shape,
+               "sort_plan": sort_plan,
                "cpu_baseline": cpu}
     print("bench-details: " + json.dumps(details), flush=True)
 
