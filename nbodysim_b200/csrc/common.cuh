@@ -15,9 +15,39 @@
 #pragma once
 
 #include <cstdint>
+#include <utility>
 #include <cuda_runtime.h>
 
 namespace nbody {
+
+// Programmatic dependent launch (sm_90 and later). The kernels of a force pass
+// and a step are launched with launch_pdl: the next kernel in the stream may be
+// scheduled while the previous one drains, and every such kernel first waits in
+// griddep_wait() until the previous kernel has completed and its memory is
+// visible (so it reads nothing of it too early), then lets the kernel after it
+// be scheduled (griddep_launch). Launched without the attribute, both are no-ops.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void griddep() {
+    griddep_wait();
+    griddep_launch();
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 constexpr double kG = 6.67384e-11;  // src/main.cpp:322
 constexpr int kLevelsPerWord = 21;  // 63 key bits per 64-bit word, 3 bits per octree level

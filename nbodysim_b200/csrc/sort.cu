@@ -10,6 +10,7 @@
 // as an error), and scatters: the tile is first laid out in digit order in
 // shared memory, so that each digit's run goes out in coalesced writes.
 #include "sort.cuh"
+#include "common.cuh"
 
 namespace nbody {
 
@@ -28,6 +29,7 @@ constexpr uint32_t kSpinLimit = 1u << 20;
 __global__ void k_hist(const uint64_t *__restrict__ wa, int pa, int slot_a, const uint64_t *__restrict__ wb, int pb,
                        int slot_b, const uint32_t *__restrict__ wc, int slot_c, uint32_t n,
                        uint32_t *__restrict__ ghist, const uint32_t *run_if) {
+    griddep();
     __shared__ uint32_t s_h[18 * 256];
     if (run_if && *run_if == 0u) return;
     const int pc = wc ? 2 : 0, np = pa + pb + pc;
@@ -56,9 +58,19 @@ __global__ void k_hist(const uint64_t *__restrict__ wa, int pa, int slot_a, cons
     }
 }
 
+// Zeroes `words` 32-bit words (16-byte aligned), four per thread and step.
+__global__ void k_zero_words(uint32_t *__restrict__ p, size_t words) {
+    griddep();
+    const size_t q = words / 4, stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = blockIdx.x * blockDim.x + threadIdx.x; i < q; i += stride)
+        reinterpret_cast<uint4 *>(p)[i] = make_uint4(0u, 0u, 0u, 0u);
+    for (size_t i = 4 * q + blockIdx.x * blockDim.x + threadIdx.x; i < words; i += stride) p[i] = 0u;
+}
+
 // Exclusive scan of each pass's 256 counts (one block per pass, in the order of k_hist).
 __global__ void k_hist_scan(uint32_t *__restrict__ ghist, int pa, int slot_a, int pb, int slot_b, int slot_c,
                             const uint32_t *run_if) {
+    griddep();
     __shared__ uint32_t s[256];
     if (run_if && *run_if == 0u) return;
     const int k = blockIdx.x;
@@ -83,6 +95,7 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint64_t *__restric
                                                        const uint32_t *__restrict__ goff, uint32_t *status,
                                                        uint32_t *ticket, uint32_t *err, uint32_t err_bit,
                                                        const uint32_t *run_if) {
+    griddep();
     __shared__ uint32_t s_wc[kWarps][256];  // per-warp digit counts, then per-warp offsets
     __shared__ uint32_t s_base[256];        // global position of the tile's first key of each digit
     __shared__ uint32_t s_lstart[256];      // position of each digit's first key within the tile
@@ -226,7 +239,9 @@ size_t sort_scratch_bytes(uint32_t n) {
 }
 
 cudaError_t sort_reset(uint32_t *scratch, uint32_t n, cudaStream_t st) {
-    return cudaMemsetAsync(scratch, 0, sort_scratch_bytes(n), st);
+    const size_t words = sort_scratch_bytes(n) / 4;
+    const unsigned blocks = (unsigned)std::min<size_t>(1184, (words / 4 + 255) / 256);
+    return launch_pdl(k_zero_words, dim3(blocks ? blocks : 1), dim3(256), 0, st, scratch, words);
 }
 
 cudaError_t sort_histograms(const uint64_t *wa, int pa, int slot_a, const uint64_t *wb, int pb, int slot_b,
@@ -237,8 +252,8 @@ cudaError_t sort_histograms(const uint64_t *wa, int pa, int slot_a, const uint64
     const int np = pa + pb + (wc ? 2 : 0);
     if (np == 0) return cudaSuccess;
     const unsigned blocks = (unsigned)std::min<size_t>(1184, (n + 255) / 256);
-    k_hist<<<blocks ? blocks : 1, 256, 0, st>>>(wa, pa, slot_a, wb, pb, slot_b, wc, slot_c, n, scratch, run_if);
-    k_hist_scan<<<np, 256, 0, st>>>(scratch, pa, slot_a, pb, slot_b, slot_c, run_if);
+    launch_pdl(k_hist, dim3(blocks ? blocks : 1), dim3(256), 0, st, wa, pa, slot_a, wb, pb, slot_b, wc, slot_c, n, scratch, run_if);
+    launch_pdl(k_hist_scan, dim3(np), dim3(256), 0, st, scratch, pa, slot_a, pb, slot_b, slot_c, run_if);
     *launches += 2;
     return cudaGetLastError();
 }
@@ -250,7 +265,7 @@ cudaError_t sort_pass(const uint64_t *kin, const uint32_t *iin, uint64_t *kout, 
     uint32_t *goff = scratch + 256 * slot;
     uint32_t *status = scratch + kSortSlots * 256 + (size_t)slot * tiles * 256;
     uint32_t *ticket = scratch + kSortSlots * 256 + kSortSlots * tiles * 256 + slot;
-    k_onesweep<<<(unsigned)tiles, kThreads, 0, st>>>(kin, iin, kout, iout, n, shift, goff, status, ticket, err,
+    launch_pdl(k_onesweep, dim3((unsigned)tiles), dim3(kThreads), 0, st, kin, iin, kout, iout, n, shift, goff, status, ticket, err,
                                                      err_bit, run_if);
     *launches += 1;
     return cudaGetLastError();

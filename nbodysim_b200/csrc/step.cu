@@ -16,6 +16,7 @@ namespace nbody {
 template <typename AccT>
 __global__ void k_update(double *__restrict__ pos, double *__restrict__ vel, const AccT *__restrict__ acc,
                          uint32_t n, StepParams sp, DevScalars *sc) {
+    griddep();
     double dt = sp.dt;
     if (sp.adaptive) {
         const double amax = __longlong_as_double((long long)sc->max_acc_bits);
@@ -56,6 +57,7 @@ __global__ void k_update(double *__restrict__ pos, double *__restrict__ vel, con
 __global__ void k_diag(const double *__restrict__ pos, const double *__restrict__ vel,
                        const double *__restrict__ mass, const double *__restrict__ pot, uint32_t n,
                        double *__restrict__ partial, DevScalars *sc) {
+    griddep();
     constexpr int K = kDiagCount;
     __shared__ double s_red[K][32];
     __shared__ bool s_last;
@@ -105,6 +107,7 @@ __global__ void k_diag(const double *__restrict__ pos, const double *__restrict_
 }
 
 __global__ void k_reset_pass(DevScalars *sc) {
+    griddep();
     sc->interactions = 0;
     sc->walk_entries = 0;
     sc->walk_tiles = 0;
@@ -125,6 +128,7 @@ __global__ void k_reset_pass(DevScalars *sc) {
 }
 
 __global__ void k_acc_to_double(const float *__restrict__ in, double *__restrict__ out, size_t count) {
+    griddep();
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < count) out[i] = (double)in[i];
 }
@@ -135,6 +139,7 @@ __global__ void k_acc_to_double(const float *__restrict__ in, double *__restrict
 //   mu = lv' + lx' dt;  lv = mu;  la = mu dt;  lx = lx' + (dF/dx)^T la.
 __global__ void k_adj_pre(const double *__restrict__ lx, double *__restrict__ lv, double *__restrict__ lam, double dt,
                           uint32_t n) {
+    griddep();
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= 3 * (size_t)n) return;
     const double mu = lv[i] + lx[i] * dt;
@@ -152,6 +157,7 @@ __global__ void k_adj_distribute(const double4 *__restrict__ body, const uint32_
                                  const double *__restrict__ adj_leaf, const GT *__restrict__ gdir,
                                  const double *__restrict__ scale, double *__restrict__ lx, double *__restrict__ lm,
                                  uint32_t n) {
+    griddep();
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     const uint32_t ui = sidx[j];
@@ -182,7 +188,7 @@ __global__ void k_adj_distribute(const double4 *__restrict__ body, const uint32_
 
 cudaError_t launch_adj_pre(const double *lx, double *lv, double *lam, double dt, uint32_t n, cudaStream_t st) {
     const unsigned blocks = (unsigned)((3 * (size_t)n + 255) / 256);
-    k_adj_pre<<<blocks, 256, 0, st>>>(lx, lv, lam, dt, n);
+    launch_pdl(k_adj_pre, dim3(blocks), dim3(256), 0, st, lx, lv, lam, dt, n);
     return cudaGetLastError();
 }
 
@@ -192,16 +198,17 @@ cudaError_t launch_adj_distribute(const double4 *body, const uint32_t *sidx, con
                                   double *lx, double *lm, uint32_t n, cudaStream_t st) {
     const unsigned blocks = (n + 255) / 256;
     if (gdir_double)
-        k_adj_distribute<double><<<blocks, 256, 0, st>>>(body, sidx, leaf_oparent, oparent, onode, adj_node, adj_leaf,
+        launch_pdl(k_adj_distribute<double>, dim3(blocks), dim3(256), 0, st, body, sidx, leaf_oparent, oparent, onode, adj_node, adj_leaf,
                                                          (const double *)gdir, scale, lx, lm, n);
     else
-        k_adj_distribute<float><<<blocks, 256, 0, st>>>(body, sidx, leaf_oparent, oparent, onode, adj_node, adj_leaf,
+        launch_pdl(k_adj_distribute<float>, dim3(blocks), dim3(256), 0, st, body, sidx, leaf_oparent, oparent, onode, adj_node, adj_leaf,
                                                         (const float *)gdir, scale, lx, lm, n);
     return cudaGetLastError();
 }
 
 // Largest |v| over count doubles, into *out (ordered bits of a non-negative double).
 __global__ void k_absmax(const double *__restrict__ v, size_t count, unsigned long long *out) {
+    griddep();
     __shared__ double s_w[32];
     double m = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x)
@@ -221,6 +228,7 @@ __global__ void k_absmax(const double *__restrict__ v, size_t count, unsigned lo
 // (e = 0 when it is zero or not finite); sc->lam_scale = 2^e.
 __global__ void k_scale_to_float(const double *__restrict__ in, float *__restrict__ out, size_t count,
                                  DevScalars *sc) {
+    griddep();
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const double mx = __longlong_as_double((long long)sc->lam_max_bits);
     int e = 0;
@@ -233,9 +241,9 @@ cudaError_t launch_lam_to_float_scaled(const double *in, float *out, size_t coun
     cudaError_t e = cudaMemsetAsync(&sc->lam_max_bits, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
     const size_t blocks = (count + 255) / 256;
-    k_absmax<<<(unsigned)std::max<size_t>(1, std::min<size_t>(blocks, 1184)), 256, 0, st>>>(in, count,
+    launch_pdl(k_absmax, dim3((unsigned)std::max<size_t>(1, std::min<size_t>(blocks, 1184))), dim3(256), 0, st, in, count,
                                                                                          &sc->lam_max_bits);
-    k_scale_to_float<<<(unsigned)std::max<size_t>(1, blocks), 256, 0, st>>>(in, out, count, sc);
+    launch_pdl(k_scale_to_float, dim3((unsigned)std::max<size_t>(1, blocks)), dim3(256), 0, st, in, out, count, sc);
     return cudaGetLastError();
 }
 
@@ -243,15 +251,15 @@ cudaError_t launch_update(double *pos, double *vel, const void *acc, bool acc_do
                           const StepParams &sp, DevScalars *sc, cudaStream_t st) {
     const unsigned blocks = n ? (n + 255) / 256 : 1;
     if (acc_double)
-        k_update<double><<<blocks, 256, 0, st>>>(pos, vel, (const double *)acc, n, sp, sc);
+        launch_pdl(k_update<double>, dim3(blocks), dim3(256), 0, st, pos, vel, (const double *)acc, n, sp, sc);
     else
-        k_update<float><<<blocks, 256, 0, st>>>(pos, vel, (const float *)acc, n, sp, sc);
+        launch_pdl(k_update<float>, dim3(blocks), dim3(256), 0, st, pos, vel, (const float *)acc, n, sp, sc);
     return cudaGetLastError();
 }
 
 cudaError_t launch_diag(const double *pos, const double *vel, const double *mass, const double *pot,
                         uint32_t n, double *partial, unsigned blocks, DevScalars *sc, cudaStream_t st) {
-    k_diag<<<blocks, 256, 0, st>>>(pos, vel, mass, pot, n, partial, sc);
+    launch_pdl(k_diag, dim3(blocks), dim3(256), 0, st, pos, vel, mass, pot, n, partial, sc);
     return cudaGetLastError();
 }
 
@@ -260,6 +268,7 @@ cudaError_t launch_diag(const double *pos, const double *vel, const double *mass
 // velocities arrive after the force pass).
 template <typename AccT>
 __global__ void k_maxima(const AccT *__restrict__ acc, const double *__restrict__ vel, uint32_t n, DevScalars *sc) {
+    griddep();
     double amax = 0.0, vmax = 0.0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const size_t o = 3 * (size_t)i;
@@ -282,19 +291,19 @@ cudaError_t launch_maxima(const void *acc, bool acc_double, const double *vel, u
     if (e == cudaSuccess) e = cudaMemsetAsync(&sc->max_vel_bits, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess || n == 0) return e;
     const unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 592);
-    if (acc_double) k_maxima<double><<<blocks, 256, 0, st>>>((const double *)acc, vel, n, sc);
-    else k_maxima<float><<<blocks, 256, 0, st>>>((const float *)acc, vel, n, sc);
+    if (acc_double) launch_pdl(k_maxima<double>, dim3(blocks), dim3(256), 0, st, (const double *)acc, vel, n, sc);
+    else launch_pdl(k_maxima<float>, dim3(blocks), dim3(256), 0, st, (const float *)acc, vel, n, sc);
     return cudaGetLastError();
 }
 
 cudaError_t launch_reset_pass(DevScalars *sc, cudaStream_t st) {
-    k_reset_pass<<<1, 1, 0, st>>>(sc);
+    launch_pdl(k_reset_pass, dim3(1), dim3(1), 0, st, sc);
     return cudaGetLastError();
 }
 
 cudaError_t launch_acc_to_double(const float *in, double *out, size_t count, cudaStream_t st) {
     if (!count) return cudaSuccess;
-    k_acc_to_double<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(in, out, count);
+    launch_pdl(k_acc_to_double, dim3((unsigned)((count + 255) / 256)), dim3(256), 0, st, in, out, count);
     return cudaGetLastError();
 }
 

@@ -49,6 +49,7 @@ __device__ inline void root_from_extrema(const double *lo, const double *hi, boo
 // (optionally) reduces max |v| for the adaptive step.
 __global__ void k_bbox(const double *__restrict__ pos, const double *__restrict__ vel, uint32_t n,
                        double *__restrict__ partial, DevScalars *sc, int keep_root, int single) {
+    griddep();
     __shared__ double s_red[7][32];
     __shared__ bool s_last;
     double mn[3] = {INFINITY, INFINITY, INFINITY};
@@ -116,6 +117,7 @@ __global__ void k_bbox(const double *__restrict__ pos, const double *__restrict_
 __global__ void k_bbox_systems(const double *__restrict__ pos, const double *__restrict__ mass,
                                const uint32_t *__restrict__ sys_start, double *__restrict__ sys_root,
                                DevScalars *sc, int single) {
+    griddep();
     __shared__ double s_red[6][32];
     const uint32_t b0 = sys_start[blockIdx.x], b1 = sys_start[blockIdx.x + 1];
     double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -190,6 +192,7 @@ __global__ void k_keys(const double *__restrict__ pos, uint32_t n, const DevScal
                        uint64_t *__restrict__ k2_user, uint32_t *__restrict__ idx,
                        const uint32_t *__restrict__ sys_id, const double *__restrict__ sys_root, int single,
                        int sort_by_k1) {
+    griddep();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double root[4];
@@ -215,6 +218,7 @@ __global__ void k_keys(const double *__restrict__ pos, uint32_t n, const DevScal
 // without them; nothing unless *run_if is non-zero.
 __global__ void k_keys_second(const double *__restrict__ pos, uint32_t n, const DevScalars *sc,
                               uint64_t *__restrict__ k2_user, int single, const uint32_t *run_if) {
+    griddep();
     if (*run_if == 0u) return;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -229,6 +233,7 @@ __global__ void k_keys_second(const double *__restrict__ pos, uint32_t n, const 
 // dst[j] = src[idx[j]]; with run_if non-null, only when *run_if is non-zero.
 __global__ void k_gather_key(const uint64_t *__restrict__ src, const uint32_t *__restrict__ idx,
                              uint64_t *__restrict__ dst, uint32_t n, const uint32_t *run_if) {
+    griddep();
     if (run_if && *run_if == 0u) return;
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j < n) dst[j] = src[idx[j]];
@@ -241,6 +246,7 @@ __global__ void k_gather_key(const uint64_t *__restrict__ src, const uint32_t *_
 __global__ void k_prefix_ties(const uint64_t *__restrict__ k1_sorted, const uint64_t *__restrict__ k2_sorted,
                               int s1, int s2, uint32_t n, uint32_t *ties, cudaGraphConditionalHandle cond,
                               int use_cond) {
+    griddep();
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     bool tie = j + 1 < n && (k1_sorted[j] >> s1) == (k1_sorted[j + 1] >> s1);
     if (tie && k2_sorted) tie = (k2_sorted[j] >> s2) == (k2_sorted[j + 1] >> s2);
@@ -253,6 +259,7 @@ __global__ void k_prefix_ties(const uint64_t *__restrict__ k1_sorted, const uint
 // Start of the full sort after ties: the second words as sort keys, identity indices.
 __global__ void k_full_sort_init(const uint64_t *__restrict__ k2_user, uint64_t *__restrict__ key,
                                  uint32_t *__restrict__ idx, uint32_t n, const uint32_t *run_if) {
+    griddep();
     if (*run_if == 0u) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
@@ -263,6 +270,7 @@ __global__ void k_full_sort_init(const uint64_t *__restrict__ k2_user, uint64_t 
 
 __global__ void k_gather_sys(const uint32_t *__restrict__ sys_id, const uint32_t *__restrict__ idx,
                              uint64_t *__restrict__ key, uint32_t *__restrict__ sys_sorted, uint32_t n) {
+    griddep();
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     const uint32_t s = sys_id[idx[j]];
@@ -301,6 +309,7 @@ __device__ inline uint32_t block_exclusive_scan(uint32_t x, uint32_t *s_warp, ui
 }
 
 __global__ void k_scan_tiles(uint32_t *__restrict__ v, uint32_t len, uint32_t *__restrict__ tile_sums) {
+    griddep();
     __shared__ uint32_t s_warp[33];
     const uint32_t base = blockIdx.x * kScanTile + 4 * threadIdx.x;
     uint32_t x[4];
@@ -319,6 +328,7 @@ __global__ void k_scan_tiles(uint32_t *__restrict__ v, uint32_t len, uint32_t *_
 
 // One block: exclusive scan of up to a few thousand tile totals; writes the grand total.
 __global__ void k_scan_small(uint32_t *__restrict__ v, uint32_t len, uint32_t *total) {
+    griddep();
     __shared__ uint32_t s_warp[33];
     uint32_t carry = 0;
     for (uint32_t b = 0; b < len; b += blockDim.x) {
@@ -334,15 +344,16 @@ __global__ void k_scan_small(uint32_t *__restrict__ v, uint32_t len, uint32_t *t
 }
 
 __global__ void k_scan_add(uint32_t *__restrict__ v, uint32_t len, const uint32_t *__restrict__ tile_sums) {
+    griddep();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < len) v[i] += tile_sums[i / kScanTile];
 }
 
 unsigned scan_exclusive(uint32_t *v, uint32_t len, uint32_t *tile_sums, uint32_t *total, cudaStream_t st) {
     const uint32_t tiles = (len + kScanTile - 1) / kScanTile;
-    k_scan_tiles<<<tiles, kScanThreads, 0, st>>>(v, len, tile_sums);
-    k_scan_small<<<1, kScanThreads, 0, st>>>(tile_sums, tiles, total);
-    if (tiles > 1) k_scan_add<<<(len + 255) / 256, 256, 0, st>>>(v, len, tile_sums);
+    launch_pdl(k_scan_tiles, dim3(tiles), dim3(kScanThreads), 0, st, v, len, tile_sums);
+    launch_pdl(k_scan_small, dim3(1), dim3(kScanThreads), 0, st, tile_sums, tiles, total);
+    if (tiles > 1) launch_pdl(k_scan_add, dim3((len + 255) / 256), dim3(256), 0, st, v, len, tile_sums);
     return tiles > 1 ? 3u : 2u;
 }
 
@@ -351,6 +362,7 @@ unsigned scan_exclusive(uint32_t *v, uint32_t len, uint32_t *tile_sums, uint32_t
 __global__ void k_gather_bodies(const uint32_t *__restrict__ idx, const double *__restrict__ pos,
                                 const double *__restrict__ mass, double4 *__restrict__ body,
                                 uint32_t n, DevScalars *sc, int single) {
+    griddep();
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     uint32_t i = idx[j];
@@ -373,6 +385,7 @@ __global__ void k_deep_groups(const uint64_t *__restrict__ key1, const uint64_t 
                               uint64_t *__restrict__ key3, uint32_t *__restrict__ idx,
                               double4 *__restrict__ body, uint32_t n, const uint32_t *__restrict__ sys,
                               const double *__restrict__ sys_root, DevScalars *sc, int single) {
+    griddep();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i + 1 >= n) return;
     const uint64_t k = key1[i], kk = key2[i];
@@ -449,6 +462,7 @@ __device__ inline int level_of(int delta) { return min(delta / 3, kMaxLevels); }
 __global__ void k_radix_tree(KeyView kv, int32_t *__restrict__ bleft, int32_t *__restrict__ bright,
                              int32_t *__restrict__ bparent, int32_t *__restrict__ leaf_bparent,
                              int32_t *__restrict__ bdelta, uint32_t *max_prefix_bits) {
+    griddep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = kv.n;
     // the deepest split: key bits that separate every pair of neighbours
@@ -492,22 +506,35 @@ __global__ void k_radix_tree(KeyView kv, int32_t *__restrict__ bleft, int32_t *_
 
 // A binary node heads an octree node iff it is the root or its parent sits
 // at a shallower octree level.
+// Also the starting values of the collapse and the COM climb: a copy of the
+// flags to be scanned in place (head_id), parents "none" (so that a child the
+// collapse could not attach, reported as an error, is never followed) and zero
+// arrival counts. One thread per particle (n = m + 1).
 __global__ void k_head_flags(const int32_t *__restrict__ bparent, const int32_t *__restrict__ bdelta,
-                             uint32_t m, uint32_t *__restrict__ flag) {
+                             uint32_t m, uint32_t *__restrict__ flag, uint32_t *__restrict__ head_id,
+                             int32_t *__restrict__ oparent, int32_t *__restrict__ leaf_oparent,
+                             uint32_t *__restrict__ ocount) {
+    griddep();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m) return;
-    if (bdelta[i] < 0) {  // not an internal node (the last particle of a system)
-        flag[i] = 0u;
-        return;
+    if (i > m) return;
+    leaf_oparent[i] = -1;
+    if (i == m) return;
+    oparent[i] = -1;
+    ocount[i] = 0u;
+    uint32_t f = 0u;  // not an internal node (the last particle of a system)
+    if (bdelta[i] >= 0) {
+        const int p = bparent[i];
+        f = (p < 0 || level_of(bdelta[p]) < level_of(bdelta[i])) ? 1u : 0u;
     }
-    int p = bparent[i];
-    flag[i] = (p < 0 || level_of(bdelta[p]) < level_of(bdelta[i])) ? 1u : 0u;
+    flag[i] = f;
+    head_id[i] = f;
 }
 
 // Octree root of every system: the head of the binary node at the system's
 // first particle (none for a system of fewer than two particles).
 __global__ void k_sys_roots(const uint32_t *__restrict__ sys_start, const uint32_t *__restrict__ flag,
                             const uint32_t *__restrict__ head_id, uint32_t nsys, int32_t *__restrict__ root_node) {
+    griddep();
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nsys) return;
     const uint32_t a = sys_start[s], b = sys_start[s + 1];
@@ -522,6 +549,7 @@ __global__ void k_collapse(const int32_t *__restrict__ bleft, const int32_t *__r
                            const uint32_t *__restrict__ flag, uint32_t m, int32_t *__restrict__ ochild,
                            int32_t *__restrict__ ometa, int32_t *__restrict__ oparent,
                            int32_t *__restrict__ leaf_oparent, DevScalars *sc) {
+    griddep();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m || !flag[i]) return;
     const int id = (int)head_id[i];
@@ -631,6 +659,7 @@ __global__ void k_com(const double4 *__restrict__ body, const int32_t *__restric
                       const int32_t *__restrict__ oparent, const int32_t *__restrict__ ochild,
                       const int32_t *__restrict__ ometa, double4 *onode, uint32_t *ocount,
                       uint32_t n, DevScalars *sc) {
+    griddep();
     // One thread per node; the climb starts at nodes whose children are all
     // bodies, and a node is computed by the last of its node children to finish.
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -674,11 +703,11 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
     if (n == 0) return cudaSuccess;
     const bool multi = tb.nsys > 1;
     // root cube (+ max |v| when requested); one per system when there are several
-    k_bbox<<<tb.bbox_blocks, 256, 0, st>>>(tb.pos, tb.vel_for_max, n, tb.bbox_partial, tb.sc,
+    launch_pdl(k_bbox, dim3(tb.bbox_blocks), dim3(256), 0, st, tb.pos, tb.vel_for_max, n, tb.bbox_partial, tb.sc,
                                            multi ? 0 : tb.keep_root, tb.single);
     if (multi) {
         if (tb.mass_ready) cudaStreamWaitEvent(st, tb.mass_ready, 0);
-        k_bbox_systems<<<tb.nsys, 256, 0, st>>>(tb.pos, tb.mass, tb.sys_start, tb.sys_root, tb.sc, tb.single);
+        launch_pdl(k_bbox_systems, dim3(tb.nsys), dim3(256), 0, st, tb.pos, tb.mass, tb.sys_start, tb.sys_root, tb.sc, tb.single);
         L += 1;
     }
     uint32_t *sort_err = &tb.sc->status;
@@ -697,7 +726,7 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
         }
     };
     auto gather = [&](const uint64_t *src, uint64_t *dst, const uint32_t *run_if, cudaStream_t s) {
-        k_gather_key<<<blocks_for(n, 256), 256, 0, s>>>(src, tb.idx_a, dst, n, run_if);
+        launch_pdl(k_gather_key, dim3(blocks_for(n, 256)), dim3(256), 0, s, src, tb.idx_a, dst, n, run_if);
         L += 1;
     };
     // Slots: passes on k2 0-7, on k1 8-15, on the system id 16-17; the full sort
@@ -710,7 +739,7 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
     if (p2 > 0) {
         uint64_t *k0 = (p2 & 1) ? tb.key_b : tb.key_a, *k0o = (p2 & 1) ? tb.key_a : tb.key_b;
         uint32_t *i0 = (p2 & 1) ? tb.idx_b : tb.idx_a, *i0o = (p2 & 1) ? tb.idx_a : tb.idx_b;
-        k_keys<<<blocks_for(n, 256), 256, 0, st>>>(tb.pos, n, tb.sc, tb.key3, k0, tb.key2, i0,
+        launch_pdl(k_keys, dim3(blocks_for(n, 256)), dim3(256), 0, st, tb.pos, n, tb.sc, tb.key3, k0, tb.key2, i0,
                                                    multi ? tb.sys_id : nullptr, tb.sys_root, tb.single, 0);
         L += 1;
         cudaError_t e = sort_reset(tb.sort_scratch, n, st);
@@ -724,7 +753,7 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
     } else {
         uint64_t *k0 = (p1 & 1) ? tb.key_a : tb.key_b, *k0o = (p1 & 1) ? tb.key_b : tb.key_a;
         uint32_t *i0 = (p1 & 1) ? tb.idx_b : tb.idx_a, *i0o = (p1 & 1) ? tb.idx_a : tb.idx_b;
-        k_keys<<<blocks_for(n, 256), 256, 0, st>>>(tb.pos, n, tb.sc, tb.key3, k0, nullptr, i0, nullptr, tb.sys_root,
+        launch_pdl(k_keys, dim3(blocks_for(n, 256)), dim3(256), 0, st, tb.pos, n, tb.sc, tb.key3, k0, nullptr, i0, nullptr, tb.sys_root,
                                                    tb.single, 1);
         L += 1;
         cudaError_t e = sort_reset(tb.sort_scratch, n, st);
@@ -747,7 +776,7 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
                               cs == cudaStreamCaptureStatusActive &&
                               cudaGraphConditionalHandleCreate(&cond, cg, 0, cudaGraphCondAssignDefault) == cudaSuccess;
         if (!use_cond) cudaGetLastError();
-        k_prefix_ties<<<blocks_for(n, 256), 256, 0, st>>>(tb.key_b, p2 > 0 ? tb.key_a : nullptr,
+        launch_pdl(k_prefix_ties, dim3(blocks_for(n, 256)), dim3(256), 0, st, tb.key_b, p2 > 0 ? tb.key_a : nullptr,
                                                           p2 > 0 ? 0 : digit_shift(p1, 0), p2 > 0 ? digit_shift(p2, 0) : 0,
                                                           n, ties, cond, use_cond ? 1 : 0);
         L += 1;
@@ -773,13 +802,13 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
         }
         // the full sort by (k1, k2): 8 passes on k2, the gather of k1, 8 passes on k1
         if (p2 == 0) {
-            k_keys_second<<<blocks_for(n, 256), 256, 0, fs>>>(tb.pos, n, tb.sc, tb.key2, tb.single, ties);
+            launch_pdl(k_keys_second, dim3(blocks_for(n, 256)), dim3(256), 0, fs, tb.pos, n, tb.sc, tb.key2, tb.single, ties);
             L += 1;
         }
         if ((e = sort_histograms(tb.key2, 8, 18, tb.key3, 8, 26, nullptr, 0, n, tb.sort_scratch, ties, fs, &L)) !=
             cudaSuccess)
             return e;
-        k_full_sort_init<<<blocks_for(n, 256), 256, 0, fs>>>(tb.key2, tb.key_a, tb.idx_a, n, ties);
+        launch_pdl(k_full_sort_init, dim3(blocks_for(n, 256)), dim3(256), 0, fs, tb.key2, tb.key_a, tb.idx_a, n, ties);
         L += 1;
         passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b, 8, 8, 18, ties, fs);  // result: key_a, idx_a
         gather(tb.key3, tb.key_b, ties, fs);
@@ -792,41 +821,37 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
     }
     if (multi) {
         // then by system (16-bit ids, 2 stable passes; result back in key_a / idx_a)
-        k_gather_sys<<<blocks_for(n, 256), 256, 0, st>>>(tb.sys_id, tb.idx_a, tb.key_a, nullptr, n);
+        launch_pdl(k_gather_sys, dim3(blocks_for(n, 256)), dim3(256), 0, st, tb.sys_id, tb.idx_a, tb.key_a, nullptr, n);
         passes(tb.key_a, tb.key_b, tb.idx_a, tb.idx_b, 2, 8, 16, nullptr, st);
         gather(tb.key3, tb.key_b, nullptr, st);  // k1 sorted
-        k_gather_sys<<<blocks_for(n, 256), 256, 0, st>>>(tb.sys_id, tb.idx_a, nullptr, tb.sys_sorted, n);
+        launch_pdl(k_gather_sys, dim3(blocks_for(n, 256)), dim3(256), 0, st, tb.sys_id, tb.idx_a, nullptr, tb.sys_sorted, n);
         L += 2;
     }
     // k2 sorted into key_a (a checked plan has it already, or needs none: with
     // every k1 prefix distinct, nothing reads k2)
     if (!checked) gather(tb.key2, tb.key_a, nullptr, st);
     if (tb.mass_ready && !multi) cudaStreamWaitEvent(st, tb.mass_ready, 0);  // the first reader of the masses
-    k_gather_bodies<<<blocks_for(n, 256), 256, 0, st>>>(tb.idx_a, tb.pos, tb.mass, tb.body, n, tb.sc, tb.single);
+    launch_pdl(k_gather_bodies, dim3(blocks_for(n, 256)), dim3(256), 0, st, tb.idx_a, tb.pos, tb.mass, tb.body, n, tb.sc, tb.single);
     L += 1;
     *launches += L;
     if (n < 2) return cudaGetLastError();
     L = 0;
     const uint32_t *sys_sorted = multi ? tb.sys_sorted : nullptr;
-    k_deep_groups<<<blocks_for(n, 256), 256, 0, st>>>(tb.key_b, tb.key_a, tb.key3, tb.idx_a, tb.body, n,
+    launch_pdl(k_deep_groups, dim3(blocks_for(n, 256)), dim3(256), 0, st, tb.key_b, tb.key_a, tb.key3, tb.idx_a, tb.body, n,
                                                        sys_sorted, tb.sys_root, tb.sc, tb.single);
     KeyView kv{tb.key_b, tb.key_a, tb.key3, (int)n, sys_sorted};
     const uint32_t m = n - 1;
-    k_radix_tree<<<blocks_for(m, 256), 256, 0, st>>>(kv, tb.bleft, tb.bright, tb.bparent, tb.leaf_bparent,
+    launch_pdl(k_radix_tree, dim3(blocks_for(m, 256)), dim3(256), 0, st, kv, tb.bleft, tb.bright, tb.bparent, tb.leaf_bparent,
                                                       tb.bdelta, &tb.sc->max_prefix_bits);
-    k_head_flags<<<blocks_for(m, 256), 256, 0, st>>>(tb.bparent, tb.bdelta, m, tb.head_flag);
-    cudaMemcpyAsync(tb.head_id, tb.head_flag, sizeof(uint32_t) * m, cudaMemcpyDeviceToDevice, st);
+    launch_pdl(k_head_flags, dim3(blocks_for(n, 256)), dim3(256), 0, st, tb.bparent, tb.bdelta, m, tb.head_flag,
+               tb.head_id, tb.oparent, tb.leaf_oparent, tb.ocount);
     L += 3 + scan_exclusive(tb.head_id, m, tb.scan_tmp, &tb.sc->n_onodes, st);
-    // Parents default to "none" so a child the collapse could not attach
-    // (reported as an error) is never followed.
-    cudaMemsetAsync(tb.oparent, 0xff, sizeof(int32_t) * m, st);
-    cudaMemsetAsync(tb.leaf_oparent, 0xff, sizeof(int32_t) * n, st);
-    k_collapse<<<blocks_for(m, 256), 256, 0, st>>>(tb.bleft, tb.bright, tb.bdelta, tb.head_id, tb.head_flag,
+    launch_pdl(k_collapse, dim3(blocks_for(m, 256)), dim3(256), 0, st, tb.bleft, tb.bright, tb.bdelta, tb.head_id, tb.head_flag,
                                                     m, tb.ochild, tb.ometa, tb.oparent, tb.leaf_oparent,
                                                     tb.sc);
     L += 1;
     if (multi) {
-        k_sys_roots<<<blocks_for(tb.nsys, 256), 256, 0, st>>>(tb.sys_start, tb.head_flag, tb.head_id, tb.nsys,
+        launch_pdl(k_sys_roots, dim3(blocks_for(tb.nsys, 256)), dim3(256), 0, st, tb.sys_start, tb.head_flag, tb.head_id, tb.nsys,
                                                                tb.sys_root_node);
         L += 1;
     }
@@ -837,13 +862,12 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
 cudaError_t compute_com(const TreeBuild &tb, cudaStream_t st, unsigned *launches) {
     const uint32_t n = tb.n;
     if (n < 2) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(tb.ocount, 0, sizeof(uint32_t) * (n - 1), st);
-    if (e != cudaSuccess) return e;
+    // (the arrival counts were zeroed by the build's k_head_flags)
     if (tb.single)
-        k_com<float><<<blocks_for(n - 1, 256), 256, 0, st>>>(tb.body, tb.leaf_oparent, tb.oparent, tb.ochild,
+        launch_pdl(k_com<float>, dim3(blocks_for(n - 1, 256)), dim3(256), 0, st, tb.body, tb.leaf_oparent, tb.oparent, tb.ochild,
                                                              tb.ometa, tb.onode, tb.ocount, n, tb.sc);
     else
-        k_com<double><<<blocks_for(n - 1, 256), 256, 0, st>>>(tb.body, tb.leaf_oparent, tb.oparent, tb.ochild,
+        launch_pdl(k_com<double>, dim3(blocks_for(n - 1, 256)), dim3(256), 0, st, tb.body, tb.leaf_oparent, tb.oparent, tb.ochild,
                                                               tb.ometa, tb.onode, tb.ocount, n, tb.sc);
     *launches += 1;
     return cudaGetLastError();

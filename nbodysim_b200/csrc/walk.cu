@@ -488,6 +488,7 @@ __device__ inline void flush_list(Sm &s, int count, int lane, const WalkArgs &a,
 template <bool kFp64, bool kDamp, bool kPot, bool kAdj>
 __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    griddep();
     using Sm = WarpSmem<kFp64>;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     Sm &s = reinterpret_cast<Sm *>(smem_raw)[wid];
@@ -1019,7 +1020,17 @@ cudaError_t launch_walk(const WalkArgs &a, bool fp64, const WalkLaunch &l, cudaS
     if (need < blocks) blocks = need ? need : 1;
     WalkArgs args = a;
     void *params[] = {&args};
-    return cudaLaunchKernel(k, dim3(blocks), dim3(l.warps * 32), params, l.smem, st);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(l.warps * 32);
+    cfg.dynamicSmemBytes = l.smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, k, params);
 }
 
 }  // namespace nbody
