@@ -3,7 +3,8 @@
 // The global digit counts of every pass do not depend on the order of the
 // keys, so one kernel computes them for all passes up front. Each pass then
 // is a single kernel: a block takes the next tile (4096 keys) in ticket order,
-// ranks its keys stably (per warp, match_any over 16 rounds of 32 keys),
+// ranks its keys stably (per warp, 16 rounds of 32 keys; the lanes that share
+// a digit are found with eight ballots, one per digit bit),
 // publishes its per-digit count, adds the counts of all earlier tiles by
 // decoupled look-back (a tile only ever waits for tiles that started before
 // it, so the wait always ends; it is still bounded, and a timeout is reported
@@ -112,15 +113,26 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint64_t *__restric
     const uint32_t lt = (1u << lane) - 1u;
     uint64_t key[kItems];
     uint32_t idx[kItems], rank[kItems];
-    // ---- load and rank: warp w owns keys [base, base + 512) in order
+    // ---- load, then rank: warp w owns keys [base, base + 512) in order
 #pragma unroll
     for (int r = 0; r < kItems; r++) {
         const uint32_t i = base + r * 32 + lane;
         const bool valid = i < n;
-        key[r] = valid ? kin[i] : 0ull;
-        idx[r] = valid ? iin[i] : 0u;
+        key[r] = valid ? __ldcs(&kin[i]) : 0ull;
+        idx[r] = valid ? __ldcs(&iin[i]) : 0u;
+    }
+#pragma unroll
+    for (int r = 0; r < kItems; r++) {
+        const uint32_t i = base + r * 32 + lane;
+        const bool valid = i < n;
         const uint32_t d = (uint32_t)((key[r] >> shift) & 255u);
-        const uint32_t peers = __match_any_sync(0xffffffffu, valid ? d : 256u + lane);
+        uint32_t peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            const uint32_t bb = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+            peers &= ((d >> b) & 1u) ? bb : ~bb;
+        }
+        if (!valid) peers = 1u << lane;
         const uint32_t before = valid ? s_wc[w][d] : 0u;
         rank[r] = before + __popc(peers & lt);
         __syncwarp();
