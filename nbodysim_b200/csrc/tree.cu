@@ -64,7 +64,7 @@ __global__ void k_bbox(const double *__restrict__ pos, const double *__restrict_
         mn[2] = fmin(mn[2], z); mx[2] = fmax(mx[2], z);
         if (vel) {
             double vx = vel[3 * (size_t)i], vy = vel[3 * (size_t)i + 1], vz = vel[3 * (size_t)i + 2];
-            vmax = fmax(vmax, sqrt(vx * vx + vy * vy + vz * vz));
+            vmax = fmax(vmax, vx * vx + vy * vy + vz * vz);  // |v|^2; the square root of the maximum at the end
         }
     }
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&sc->status, kStatusNonFinite);
@@ -96,7 +96,7 @@ __global__ void k_bbox(const double *__restrict__ pos, const double *__restrict_
         r[k] = warp_min(acc);
     }
     if (lane == 0 && keep_root) {
-        sc->max_vel_bits = (unsigned long long)__double_as_longlong(-r[6]);
+        sc->max_vel_bits = (unsigned long long)__double_as_longlong(sqrt(-r[6]));
         sc->ticket = 0;
     } else if (lane == 0) {
         double lo[3] = {r[0], r[1], r[2]}, hi[3] = {-r[3], -r[4], -r[5]};
@@ -108,7 +108,7 @@ __global__ void k_bbox(const double *__restrict__ pos, const double *__restrict_
         root_from_extrema(lo, hi, single != 0, center, &side);
         for (int k = 0; k < 3; k++) sc->root_center[k] = center[k];
         sc->root_side = side;
-        sc->max_vel_bits = (unsigned long long)__double_as_longlong(-r[6]);
+        sc->max_vel_bits = (unsigned long long)__double_as_longlong(sqrt(-r[6]));
         sc->ticket = 0;
     }
 }
@@ -584,7 +584,10 @@ __global__ void k_collapse(const int32_t *__restrict__ bleft, const int32_t *__r
     }
     ometa[id] = L | (min(nch, 8) << 8) | (min(nint, 8) << 12);
     if (id == 0) oparent[0] = -1;
-    atomicMax(&sc->depth, (uint32_t)L);
+    // the deepest level: one atomic per group of converged lanes
+    const unsigned am = __activemask();
+    const uint32_t lmax = __reduce_max_sync(am, (uint32_t)L);
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(am) - 1)) atomicMax(&sc->depth, lmax);
 }
 
 // ---------------------------------------------------------------------------
