@@ -164,3 +164,21 @@ def test_step_host_on_a_caller_stream(nb):
         ref.step(2)
         p2, v2 = ref.get_particles()
     assert np.array_equal(p1, p2) and np.array_equal(v1, v2)
+
+
+@pytest.mark.parametrize("stream", [0, 2])  # the legacy default stream, the per-thread default stream
+def test_steps_on_the_default_streams(nb, stream):
+    """On the default streams the chained launches and the captured graphs give
+    the same steps as the engine's own stream (the legacy stream is launched
+    without the programmatic-dependency attribute and not captured)."""
+    import ctypes
+    pos, vel, mass = nb.generate(30000, gen_type=2, size=1024.0, seed=3)
+    with nb.Engine(adaptive=1) as e, nb.Engine(adaptive=1) as ref:
+        assert e._lib.nbody_set_stream(e._h, ctypes.c_void_p(stream)) == nb.OK
+        e.set_particles(pos, vel, mass)
+        e.step(3)
+        p1, v1 = e.get_particles()
+        ref.set_particles(pos, vel, mass)
+        ref.step(3)
+        p2, v2 = ref.get_particles()
+    assert np.array_equal(p1, p2) and np.array_equal(v1, v2)
