@@ -153,6 +153,8 @@ typedef struct nbody_stats {
     uint64_t interactions;   /* accepted (particle, node) pairs in the last force pass */
     uint64_t interactions_total; /* summed over every pass of the last API call */
     uint64_t kernel_launches;    /* kernels this context has enqueued since creation */
+    /* walk_entries .. walk_near and max_stack: collected only while
+     * nbody_set_walk_stats(ctx, 1) is on (0 otherwise) */
     uint64_t walk_entries;       /* node entries tested by the walk's warps in the last pass */
     uint64_t walk_tiles;         /* stack tiles (<= 32 entries) the walk's warps staged */
     uint64_t walk_decisions;     /* internal nodes the warps decided (open / accept) */
@@ -181,6 +183,10 @@ int nbody_get_stats(nbody_ctx *ctx, nbody_stats *out);
 /* Time phases with CUDA events on the context stream (default off; timed calls
  * launch kernels one by one). */
 int nbody_set_timing(nbody_ctx *ctx, int enabled);
+/* Collect the walk's statistics (nbody_stats walk_entries .. walk_near,
+ * max_stack; default off). The forward walk then runs its counting instance,
+ * a few % slower; forces and counts are the same either way. */
+int nbody_set_walk_stats(nbody_ctx *ctx, int enabled);
 /* Replay captured CUDA graphs for steps and adjoint steps (default on). Each
  * distinct configuration is captured on first use; a stream that cannot be
  * captured (the legacy default stream) falls back to direct launches. */

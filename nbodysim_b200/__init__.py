@@ -123,6 +123,7 @@ _SIGS = {
     "nbody_device_view_get": (C.c_int, [C.c_void_p, C.POINTER(DeviceView)]),
     "nbody_get_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "nbody_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "nbody_set_walk_stats": (C.c_int, [C.c_void_p, C.c_int]),
     "nbody_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
     "nbody_autotune": (C.c_int, [C.c_void_p]),
     "nbody_get_diagnostics": (C.c_int, [C.c_void_p, C.POINTER(Diagnostics)]),
@@ -289,6 +290,10 @@ class Engine:
 
     def set_timing(self, on: bool = True) -> None:
         _check(self._lib.nbody_set_timing(self._h, int(on)))
+
+    def set_walk_stats(self, on: bool = True) -> None:
+        """Collect the walk's statistics (stats() walk_* and max_stack)."""
+        _check(self._lib.nbody_set_walk_stats(self._h, int(on)))
 
     def barnes_hut(self, pos, mass, damping: bool = False, theta: float = 0.5, counts: bool = False):
         """Accelerations (n, 3) of every particle (the reference's barnes_hut_cuda)."""

@@ -36,6 +36,7 @@ def walk_case(args) -> None:
         if args.save:
             np.savez(args.save, pos=pos, vel=vel, mass=mass)
     with Engine(precision=1 if args.fp64 else 0) as e:
+        e.set_walk_stats(True)
         for _ in range(args.passes):
             e.barnes_hut(pos, mass, theta=args.theta)
         s = e.stats()

@@ -76,6 +76,7 @@ struct nbody_ctx {
     DevScalars *hsc = nullptr;  // pinned mirror
     WalkLaunch wl_mixed{}, wl_fp64{};
     int timing = 0;
+    int walk_stats = 0;  // nbody_set_walk_stats
     cudaEvent_t ev[5] = {};
     nbody_stats stats{};
     unsigned long long launches = 0;  // kernels enqueued by this context
@@ -367,6 +368,7 @@ int force_pass(nbody_ctx *c, int damping, double theta, bool fp64, bool want_vma
     a.sys_root_node = c->sys_root_node;
     a.sys_root = c->sys_root;
     a.track_max_acc = track_amax ? 1 : 0;
+    a.stats = c->walk_stats;
     if (adjoint) {
         a.adjoint = 1;
         a.lamf = (const float *)c->lam;
@@ -431,14 +433,14 @@ int download_acc(nbody_ctx *c, double *acc) {
 std::vector<unsigned char> graph_key(nbody_ctx *c, uint32_t extra) {
     struct K {
         uint32_t n, nsys, ngroups, extra;
-        int sort_p1, sort_p2;
+        int sort_p1, sort_p2, walk_stats;
         void *arena, *adj, *sys, *stream;
         nbody_params p;
         WalkLaunch wm, wf;
     } k;
     std::memset(&k, 0, sizeof k);
     k.n = c->n; k.nsys = c->nsys; k.ngroups = c->ngroups; k.extra = extra;
-    k.sort_p1 = c->sort_p1; k.sort_p2 = c->sort_p2;
+    k.sort_p1 = c->sort_p1; k.sort_p2 = c->sort_p2; k.walk_stats = c->walk_stats;
     k.arena = c->arena; k.adj = c->adj_arena; k.sys = c->sys_arena; k.stream = (void *)c->stream;
     k.p = c->p; k.wm = c->wl_mixed; k.wf = c->wl_fp64;
     const unsigned char *b = (const unsigned char *)&k;
@@ -1033,6 +1035,12 @@ int nbody_set_graphs(nbody_ctx *c, int enabled) {
 int nbody_set_timing(nbody_ctx *c, int enabled) {
     CTX_OR_FAIL(c);
     c->timing = enabled ? 1 : 0;
+    return NBODY_OK;
+}
+
+int nbody_set_walk_stats(nbody_ctx *c, int enabled) {
+    CTX_OR_FAIL(c);
+    c->walk_stats = enabled ? 1 : 0;
     return NBODY_OK;
 }
 

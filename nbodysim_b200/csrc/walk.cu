@@ -485,7 +485,7 @@ __device__ inline void flush_list(Sm &s, int count, int lane, const WalkArgs &a,
     if (a.counts) cnt += count_list(s.lm, count, bit);
 }
 
-template <bool kFp64, bool kDamp, bool kPot, bool kAdj>
+template <bool kFp64, bool kDamp, bool kPot, bool kAdj, bool kStats>
 __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     griddep();
@@ -577,7 +577,8 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
             s.gc.box[0] = lox; s.gc.box[1] = hix; s.gc.box[2] = loy;
             s.gc.box[3] = hiy; s.gc.box[4] = loz; s.gc.box[5] = hiz;
             s.gc.pm_tol = pm_tol; s.gc.tiny = tiny; s.gc.near_r2 = near_r2;
-            for (int q = 0; q < 6; q++) s.gc.st[q] = 0u;
+            if constexpr (kStats)
+                for (int q = 0; q < 6; q++) s.gc.st[q] = 0u;
         }
         float fax = 0.f, fay = 0.f, faz = 0.f;
         double dax = 0.0, day = 0.0, daz = 0.0, dpot = 0.0;
@@ -596,7 +597,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
             const int cntt = min(top, 32);
             const int base = top - cntt;
             top = base;
-            if (lane == 0) { s.gc.st[0] += cntt; s.gc.st[1] += 1u; }
+            if (kStats && lane == 0) { s.gc.st[0] += cntt; s.gc.st[1] += 1u; }
 
             // ---- stage: lane k takes stack entry k
             bool is_int = false;
@@ -675,7 +676,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
 
             // ---- decide the mixed nodes of the tile, lane by lane
             const uint32_t intm = __ballot_sync(FULL, mixed);
-            if (lane == 0) s.gc.st[2] += __popc(intm);
+            if (kStats && lane == 0) s.gc.st[2] += __popc(intm);
             if (intm) {
                 if constexpr (kFp64) {
                     s.tc[lane] = make_double4(cx, cy, cz, s.gc.S * so);
@@ -796,7 +797,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                 }
                 full_top += __popc(fmk);
                 list_top += __popc(pmk);
-                if (lane == 0) s.gc.st[3] += __popc(fmk) + __popc(pmk);
+                if (kStats && lane == 0) s.gc.st[3] += __popc(fmk) + __popc(pmk);
             } else {
                 const uint32_t am = __ballot_sync(FULL, accm != 0 && !near);
                 if (accm && !near) {
@@ -807,7 +808,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                     if constexpr (kAdj) s.lr[pos] = ref;
                 }
                 list_top += __popc(am);
-                if (lane == 0) s.gc.st[3] += __popc(am);
+                if (kStats && lane == 0) s.gc.st[3] += __popc(am);
             }
             if constexpr (!kFp64 && !kAdj) {
                 // forward: near bodies collect in their own paired list, offsets as hi + lo
@@ -821,7 +822,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                         s.nm[pos] = accm;
                     }
                     near_top += __popc(nmk);
-                    if (lane == 0) s.gc.st[4] += __popc(nmk);
+                    if (kStats && lane == 0) s.gc.st[4] += __popc(nmk);
                 }
             } else if constexpr (!kFp64) {
                 const uint32_t nmk = __ballot_sync(FULL, near);
@@ -836,7 +837,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                     adj_near_f32<kDamp>(s.nc, s.nm, s.nr, __popc(nmk), lane, b.x, b.y, b.z, (float)lax, (float)lay,
                                         (float)laz, fax, fay, faz, a.adj_node, a.adj_leaf);
                     if (a.counts) cnt += count_list(s.nm, __popc(nmk), 1u << lane);
-                    if (lane == 0) s.gc.st[4] += __popc(nmk);
+                    if (kStats && lane == 0) s.gc.st[4] += __popc(nmk);
                     __syncwarp();
                 }
             }
@@ -866,7 +867,7 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
                 if (myn > 6) dst[6] = make_int2(ch1.z, om);
                 if (myn > 7) dst[7] = make_int2(ch1.w, om);
                 top += total;
-                if (lane == 0) s.gc.st[5] = max(s.gc.st[5], (uint32_t)(top + (int)spill_top));
+                if (kStats && lane == 0) s.gc.st[5] = max(s.gc.st[5], (uint32_t)(top + (int)spill_top));
             }
             __syncwarp();
 
@@ -943,35 +944,45 @@ __global__ void __launch_bounds__(kWalkMaxWarps * 32) k_walk(WalkArgs a) {
             atomicAdd(&t.sc->interactions, wc);
             atomicAdd(&t.sc->interactions_total, wc);
             if (wf) atomicAdd(&t.sc->fallback_tests, wf);
-            atomicAdd(&t.sc->walk_entries, (unsigned long long)s.gc.st[0]);
-            atomicAdd(&t.sc->walk_tiles, (unsigned long long)s.gc.st[1]);
-            atomicAdd(&t.sc->walk_decisions, (unsigned long long)s.gc.st[2]);
-            atomicAdd(&t.sc->walk_list, (unsigned long long)s.gc.st[3]);
-            if (s.gc.st[4]) atomicAdd(&t.sc->walk_near, (unsigned long long)s.gc.st[4]);
-            atomicMax(&t.sc->max_stack, s.gc.st[5]);
+            if constexpr (kStats) {
+                atomicAdd(&t.sc->walk_entries, (unsigned long long)s.gc.st[0]);
+                atomicAdd(&t.sc->walk_tiles, (unsigned long long)s.gc.st[1]);
+                atomicAdd(&t.sc->walk_decisions, (unsigned long long)s.gc.st[2]);
+                atomicAdd(&t.sc->walk_list, (unsigned long long)s.gc.st[3]);
+                if (s.gc.st[4]) atomicAdd(&t.sc->walk_near, (unsigned long long)s.gc.st[4]);
+                atomicMax(&t.sc->max_stack, s.gc.st[5]);
+            }
             if (!kAdj && a.track_max_acc) atomic_max_nonneg(&t.sc->max_acc_bits, amag);
         }
     }
 }
 
-// Potentials (diagnostics) are summed by the FP64 form only.
-template <bool kFp64, bool kAdj>
-const void *walk_kernel(int damping, bool pot) {
-    if constexpr (!kFp64 && !kAdj) {
+// Potentials (diagnostics) are summed by the FP64 form only. The walk's
+// statistics (entries, tiles, decisions, list and near entries, deepest stack)
+// are collected by their own instances of the forward kernel (kStats), so that
+// the others carry none of that bookkeeping; the adjoint collects none.
+template <bool kFp64, bool kStats>
+const void *forward_kernel(int damping, bool pot) {
+    if constexpr (!kFp64) {
         (void)pot;
-        return damping ? (const void *)k_walk<false, true, false, false> : (const void *)k_walk<false, false, false, false>;
-    } else if constexpr (kAdj) {
-        return damping ? (const void *)k_walk<kFp64, true, false, true> : (const void *)k_walk<kFp64, false, false, true>;
+        return damping ? (const void *)k_walk<false, true, false, false, kStats>
+                       : (const void *)k_walk<false, false, false, false, kStats>;
     } else {
         if (damping)
-            return pot ? (const void *)k_walk<kFp64, true, true, false> : (const void *)k_walk<kFp64, true, false, false>;
-        return pot ? (const void *)k_walk<kFp64, false, true, false> : (const void *)k_walk<kFp64, false, false, false>;
+            return pot ? (const void *)k_walk<true, true, true, false, kStats>
+                       : (const void *)k_walk<true, true, false, false, kStats>;
+        return pot ? (const void *)k_walk<true, false, true, false, kStats>
+                   : (const void *)k_walk<true, false, false, false, kStats>;
     }
 }
 
-const void *any_walk_kernel(bool fp64, bool adj, int damping, bool pot) {
-    if (fp64) return adj ? walk_kernel<true, true>(damping, pot) : walk_kernel<true, false>(damping, pot);
-    return adj ? walk_kernel<false, true>(damping, pot) : walk_kernel<false, false>(damping, pot);
+const void *any_walk_kernel(bool fp64, bool adj, int damping, bool pot, bool stats) {
+    if (adj) {
+        if (fp64) return damping ? (const void *)k_walk<true, true, false, true, false> : (const void *)k_walk<true, false, false, true, false>;
+        return damping ? (const void *)k_walk<false, true, false, true, false> : (const void *)k_walk<false, false, false, true, false>;
+    }
+    if (fp64) return stats ? forward_kernel<true, true>(damping, pot) : forward_kernel<true, false>(damping, pot);
+    return stats ? forward_kernel<false, true>(damping, pot) : forward_kernel<false, false>(damping, pot);
 }
 
 }  // namespace
@@ -984,16 +995,17 @@ cudaError_t walk_max_blocks_per_sm(bool fp64, unsigned warps, int *out) {
     int minblocks = 1 << 30;
     for (int adj = 0; adj < 2; adj++)
         for (int damp = 0; damp < 2; damp++)
-            for (int pot = 0; pot < 2 - adj; pot++) {
-                const void *k = any_walk_kernel(fp64, adj, damp, pot);
-                cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     (int)(kLargestWarpSmem * kWalkMaxWarps));
-                if (e != cudaSuccess) return e;
-                int nb = 0;
-                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, (int)warps * 32, smem);
-                if (e != cudaSuccess) return e;
-                minblocks = nb < minblocks ? nb : minblocks;
-            }
+            for (int pot = 0; pot < 2 - adj; pot++)
+                for (int stats = 0; stats < 2 - adj; stats++) {
+                    const void *k = any_walk_kernel(fp64, adj, damp, pot, stats);
+                    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                         (int)(kLargestWarpSmem * kWalkMaxWarps));
+                    if (e != cudaSuccess) return e;
+                    int nb = 0;
+                    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, (int)warps * 32, smem);
+                    if (e != cudaSuccess) return e;
+                    minblocks = nb < minblocks ? nb : minblocks;
+                }
     *out = minblocks;
     return cudaSuccess;
 }
@@ -1014,7 +1026,7 @@ cudaError_t walk_launch_shape(bool fp64, int device, unsigned warps, unsigned bl
 }
 
 cudaError_t launch_walk(const WalkArgs &a, bool fp64, const WalkLaunch &l, cudaStream_t st) {
-    const void *k = any_walk_kernel(fp64, a.adjoint != 0, a.damping, a.pot != nullptr);
+    const void *k = any_walk_kernel(fp64, a.adjoint != 0, a.damping, a.pot != nullptr, a.stats != 0);
     unsigned blocks = l.blocks;
     const unsigned need = (a.n_groups + l.warps - 1) / l.warps;
     if (need < blocks) blocks = need ? need : 1;

@@ -30,6 +30,7 @@ struct WalkArgs {
     uint32_t spill_cap;
     uint32_t n_groups;  // ceil(n / 32)
     int track_max_acc;  // reduce max |a| (adaptive dt)
+    int stats;          // collect the walk statistics (DevScalars walk_* and max_stack)
     // Adjoint mode (frozen decisions): the walk computes, for the cotangent
     // lam (dL/da per particle, user order), the direct term
     // gdir_i = -sum_n K_in lam_i and the node sums adj[n] = (sum_i K_in lam_i,

@@ -182,3 +182,20 @@ def test_steps_on_the_default_streams(nb, stream):
         ref.step(3)
         p2, v2 = ref.get_particles()
     assert np.array_equal(p1, p2) and np.array_equal(v1, v2)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_walk_stats_switch_keeps_results(nb, precision):
+    """The walk's statistics come from their own kernel instance, switched on by
+    nbody_set_walk_stats: forces and counts are the same with and without it."""
+    pos, _, mass = nb.generate(20000, gen_type=2, size=1024.0, seed=11)
+    with nb.Engine(precision=precision) as e:
+        a0, c0 = e.barnes_hut(pos, mass, counts=True)
+        s0 = e.stats()
+        assert s0["walk_entries"] == 0 and s0["walk_tiles"] == 0 and s0["max_stack"] == 0
+        e.set_walk_stats(True)
+        a1, c1 = e.barnes_hut(pos, mass, counts=True)
+        s1 = e.stats()
+        assert s1["walk_entries"] > 0 and s1["walk_tiles"] > 0 and s1["walk_list"] > 0 and s1["max_stack"] > 0
+        assert s1["interactions"] == s0["interactions"] == int(c0.sum())
+    assert np.array_equal(a0, a1) and np.array_equal(c0, c1)
