@@ -36,7 +36,7 @@ def walk_case(args) -> None:
         if args.save:
             np.savez(args.save, pos=pos, vel=vel, mass=mass)
     with Engine(precision=1 if args.fp64 else 0) as e:
-        e.set_walk_stats(True)
+        e.set_walk_stats(not args.no_walk_stats)
         for _ in range(args.passes):
             e.barnes_hut(pos, mass, theta=args.theta)
         s = e.stats()
@@ -70,6 +70,8 @@ def main() -> None:
     w.add_argument("--passes", type=int, default=2)
     w.add_argument("--theta", type=float, default=0.5)
     w.add_argument("--fp64", action="store_true")
+    w.add_argument("--no-walk-stats", action="store_true",
+                   help="run the walk the bench runs (no statistics instance; the printed walk_* are then 0)")
     a = sub.add_parser("adjoint")
     a.add_argument("--n", type=int, default=65536)
     a.add_argument("--steps", type=int, default=256)
