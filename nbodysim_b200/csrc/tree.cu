@@ -617,8 +617,13 @@ template <typename T>
 __device__ inline double4 node_com(const double4 *__restrict__ body, const int32_t *__restrict__ ochild,
                                    const int32_t *__restrict__ ometa, const double4 *onode, int p, int L, int nch) {
     T m = 0, sx = 0, sy = 0, sz = 0;
+    // the child list in two 16-byte loads, so that each child's values are one load away
+    const int4 *cp = reinterpret_cast<const int4 *>(ochild + 8 * (size_t)p);
+    const int4 c0 = cp[0];
+    const int4 c1 = nch > 4 ? cp[1] : make_int4(0, 0, 0, 0);
     for (int k = 0; k < nch; k++) {
-        const int c = ochild[8 * p + k];
+        const int4 h = k < 4 ? c0 : c1;  // selects, not an indexed array (which would live in local memory)
+        const int c = (k & 2) ? ((k & 1) ? h.w : h.z) : ((k & 1) ? h.y : h.x);
         T cmk, cx, cy, cz;
         if (c < 0) {
             const double4 b = body[~c];
@@ -658,10 +663,11 @@ __device__ inline double4 node_com(const double4 *__restrict__ body, const int32
 }
 
 template <typename T>
-__global__ void k_com(const double4 *__restrict__ body, const int32_t *__restrict__ leaf_oparent,
-                      const int32_t *__restrict__ oparent, const int32_t *__restrict__ ochild,
-                      const int32_t *__restrict__ ometa, double4 *onode, uint32_t *ocount,
-                      uint32_t n, DevScalars *sc) {
+// (launch bounds: 4 resident blocks of 256 threads, 64 registers)
+__global__ void __launch_bounds__(256, 4)
+    k_com(const double4 *__restrict__ body, const int32_t *__restrict__ leaf_oparent,
+          const int32_t *__restrict__ oparent, const int32_t *__restrict__ ochild,
+          const int32_t *__restrict__ ometa, double4 *onode, uint32_t *ocount, uint32_t n, DevScalars *sc) {
     griddep();
     // One thread per node; the climb starts at nodes whose children are all
     // bodies, and a node is computed by the last of its node children to finish.
