@@ -38,8 +38,9 @@
 extern "C" {
 #endif
 
-#define NBODY_ABI_VERSION 5  /* 2: nbody_params.autotune, nbody_stats walk fields; 3: merging;
-                                4: nbody_params.datatype_bytes; 5: nbody_stats sort fields */
+#define NBODY_ABI_VERSION 6  /* 2: nbody_params.autotune, nbody_stats walk fields; 3: merging;
+                                4: nbody_params.datatype_bytes; 5: nbody_stats sort fields;
+                                6: nbody_stats.sort_tie_runs, nbody_set_walk_stats */
 
 /* ---- status codes ---------------------------------------------------- */
 #define NBODY_OK 0
@@ -174,10 +175,12 @@ typedef struct nbody_stats {
     uint64_t merged_collisions; /* particles removed by collision merges in the last nbody_step */
     uint64_t collision_pairs;  /* (particle, leaf) pairs found within range, last nbody_step */
     uint32_t sort_passes;      /* 8-bit radix-sort passes of the last tree build: the planned ones,
-                                  plus the full sort's 16 when the plan left equal neighbours */
+                                  plus the full sort's 16 when the plan left a run of more than
+                                  64 equal neighbours */
     uint32_t sort_split_bits;  /* key bits (3 per octree level) that separate every pair of
-                                  Morton neighbours in the last build; the next plan covers them
-                                  plus one level */
+                                  Morton neighbours in the last build; the next plan covers them */
+    uint32_t sort_tie_runs;    /* runs of neighbours equal over the planned bits (at most 64 each)
+                                  that the last build sorted in place */
 } nbody_stats;
 int nbody_get_stats(nbody_ctx *ctx, nbody_stats *out);
 /* Time phases with CUDA events on the context stream (default off; timed calls

@@ -224,14 +224,15 @@ int reserve(nbody_ctx *c, uint32_t n) {
 }
 
 // The next build's sort plan from the last build's deepest split (the key bits
-// that separate every pair of neighbours) plus one octree level (3 bits), in
-// whole 8-bit passes: the top bits of the first word, or all of it and the top
-// bits of the second. A plan shrinks only by two passes or more, so that small
-// changes do not rebuild captured graphs; it grows at once after a build whose
-// plan was short (it ran the full sort then). No split measured: keep the plan.
+// that separate every pair of neighbours), in whole 8-bit passes: the top bits
+// of the first word, or all of it and the top bits of the second. A plan
+// shrinks only by two passes or more, so that small changes do not rebuild
+// captured graphs; it grows at once after a build whose plan was short (it
+// sorted runs of equal neighbours in place, or ran the full sort). No split
+// measured: keep the plan.
 void next_sort_plan(nbody_ctx *c, uint32_t need_bits, bool short_plan) {
     if (need_bits == 0) return;
-    const uint32_t bits = need_bits + 3;
+    const uint32_t bits = need_bits;
     int p1 = 8, p2 = 8;
     if (bits <= 63) { p1 = (int)(bits + 7) / 8; p2 = 0; }
     else if (bits <= 126) { p2 = (int)(bits - 63 + 7) / 8; }
@@ -271,7 +272,8 @@ int check_status(nbody_ctx *c) {
     s.root_side = h.root_side;
     s.sort_passes = c->nsys > 1 ? 18u : (uint32_t)(c->sort_p1 + c->sort_p2) + (h.word_ties ? 16u : 0u);
     s.sort_split_bits = h.max_prefix_bits;
-    next_sort_plan(c, h.max_prefix_bits, h.word_ties != 0);
+    s.sort_tie_runs = h.tie_runs;
+    next_sort_plan(c, h.max_prefix_bits, h.word_ties != 0 || h.tie_runs != 0);
     if (c->timing) {
         float ms[4] = {0, 0, 0, 0};
         for (int k = 0; k < 4; k++) cudaEventElapsedTime(&ms[k], c->ev[k], c->ev[k + 1]);

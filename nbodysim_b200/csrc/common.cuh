@@ -84,7 +84,8 @@ struct DevScalars {
     uint32_t group_counter;
     uint32_t ticket;          // last-block tickets of reductions
     uint32_t deep_groups;
-    uint32_t word_ties;       // the last build's planned sort left equal neighbours (the full sort ran)
+    uint32_t word_ties;       // the last build's planned sort left a long run of equal neighbours (the full sort ran)
+    uint32_t tie_runs;        // short runs of equal neighbours the last build sorted in place
     uint32_t max_prefix_bits; // deepest split of the last build: key bits that separate every
                               // pair of neighbours (the longest common prefix + 1)
     unsigned long long max_acc_bits;  // max |a| (non-negative double as ordered bits)

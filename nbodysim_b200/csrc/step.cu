@@ -122,6 +122,7 @@ __global__ void k_reset_pass(DevScalars *sc) {
     sc->ticket = 0;
     sc->deep_groups = 0;
     sc->word_ties = 0;
+    sc->tie_runs = 0;
     sc->max_prefix_bits = 0;
     sc->max_acc_bits = 0;
     sc->max_vel_bits = 0;

@@ -239,20 +239,61 @@ __global__ void k_gather_key(const uint64_t *__restrict__ src, const uint32_t *_
     if (j < n) dst[j] = src[idx[j]];
 }
 
-// Flags equal neighbours over the bits a sort plan covered: (k1 >> s1), and
-// with k2 non-null also (k2 >> s2). Then the plan did not separate every
-// particle and the full sort is needed. Inside a captured graph (use_cond) it
-// also sets the condition of the graph node that holds the full sort.
-__global__ void k_prefix_ties(const uint64_t *__restrict__ k1_sorted, const uint64_t *__restrict__ k2_sorted,
-                              int s1, int s2, uint32_t n, uint32_t *ties, cudaGraphConditionalHandle cond,
-                              int use_cond) {
+// Runs of neighbours that the sort plan left equal over its bits, (k1 >> s1)
+// and, when the plan sorted part of the second word, (k2 >> s2), are put in
+// order here: each run of at most kMaxTieRun particles is sorted in place by
+// the full keys (k1, then k2; k2 in key_a, computed here for the run when the
+// plan had no second words), with a stable insertion sort, so that equal keys
+// keep the user order as the full LSD sort keeps it. Runs are disjoint and a
+// permutation inside a run leaves every prefix of the run unchanged, so the
+// runs are found and sorted concurrently. A longer run sets the flag of the
+// full sort (inside a captured graph, the condition of its graph node).
+constexpr uint32_t kMaxTieRun = 64;
+
+__global__ void k_fix_ties(uint64_t *__restrict__ k1_sorted, uint64_t *__restrict__ k2_sorted,
+                           uint32_t *__restrict__ idx, const double *__restrict__ pos, int have_k2, int s1, int s2,
+                           uint32_t n, int single, DevScalars *sc, cudaGraphConditionalHandle cond, int use_cond) {
     griddep();
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    bool tie = j + 1 < n && (k1_sorted[j] >> s1) == (k1_sorted[j + 1] >> s1);
-    if (tie && k2_sorted) tie = (k2_sorted[j] >> s2) == (k2_sorted[j + 1] >> s2);
-    if (__any_sync(0xffffffffu, tie) && (threadIdx.x & 31) == 0) {
-        atomicOr(ties, 1u);
-        if (use_cond) cudaGraphSetConditional(cond, 1u);
+    auto same = [&](uint32_t a, uint32_t b) {
+        bool t = (k1_sorted[a] >> s1) == (k1_sorted[b] >> s1);
+        if (t && have_k2) t = (k2_sorted[a] >> s2) == (k2_sorted[b] >> s2);
+        return t;
+    };
+    if (j + 1 >= n || !same(j, j + 1) || (j > 0 && same(j - 1, j))) return;  // not the first of a run
+    uint32_t e = j + 1;
+    while (e + 1 < n && same(e, e + 1)) {
+        if (++e - j + 1 > kMaxTieRun) {
+            atomicOr(&sc->word_ties, 1u);
+            if (use_cond) cudaGraphSetConditional(cond, 1u);
+            return;
+        }
+    }
+    atomicAdd(&sc->tie_runs, 1u);
+    if (!have_k2) {
+        const double root[4] = {sc->root_center[0], sc->root_center[1], sc->root_center[2], sc->root_side};
+        for (uint32_t q = j; q <= e; q++) {
+            const size_t u = 3 * (size_t)idx[q];
+            const double p[3] = {pos[u], pos[u + 1], pos[u + 2]};
+            uint64_t w[2];
+            if (single) descend_words<float>(p, root, 2, w);
+            else descend_words<double>(p, root, 2, w);
+            k2_sorted[q] = w[1];
+        }
+    }
+    for (uint32_t q = j + 1; q <= e; q++) {
+        const uint64_t a1 = k1_sorted[q], a2 = k2_sorted[q];
+        const uint32_t ai = idx[q];
+        uint32_t p = q;
+        while (p > j && (k1_sorted[p - 1] > a1 || (k1_sorted[p - 1] == a1 && k2_sorted[p - 1] > a2))) {
+            k1_sorted[p] = k1_sorted[p - 1];
+            k2_sorted[p] = k2_sorted[p - 1];
+            idx[p] = idx[p - 1];
+            p--;
+        }
+        k1_sorted[p] = a1;
+        k2_sorted[p] = a2;
+        idx[p] = ai;
     }
 }
 
@@ -773,11 +814,12 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
     }
     if (checked) {
         // Equal neighbours over the bits the plan sorted mean it did not separate
-        // every particle: then the full sort runs. Inside a stream capture it is
-        // the body of a conditional graph node that runs only when the check sets
-        // its condition; launched directly, each of its kernels returns at once
-        // unless the flag is set.
-        if (p2 > 0) gather(tb.key2, tb.key_a, nullptr, st);  // k2 in sorted order, for the check
+        // every particle: short runs of them are sorted in place, and a long one
+        // makes the full sort run. Inside a stream capture the full sort is the
+        // body of a conditional graph node that runs only when the check sets its
+        // condition; launched directly, each of its kernels returns at once unless
+        // the flag is set.
+        if (p2 > 0) gather(tb.key2, tb.key_a, nullptr, st);  // k2 in sorted order, for the check and the runs
         cudaGraphConditionalHandle cond = 0;
         cudaGraph_t cg = nullptr;
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -785,9 +827,9 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
                               cs == cudaStreamCaptureStatusActive &&
                               cudaGraphConditionalHandleCreate(&cond, cg, 0, cudaGraphCondAssignDefault) == cudaSuccess;
         if (!use_cond) cudaGetLastError();
-        launch_pdl(k_prefix_ties, dim3(blocks_for(n, 256)), dim3(256), 0, st, tb.key_b, p2 > 0 ? tb.key_a : nullptr,
-                                                          p2 > 0 ? 0 : digit_shift(p1, 0), p2 > 0 ? digit_shift(p2, 0) : 0,
-                                                          n, ties, cond, use_cond ? 1 : 0);
+        launch_pdl(k_fix_ties, dim3(blocks_for(n, 256)), dim3(256), 0, st, tb.key_b, tb.key_a, tb.idx_a, tb.pos,
+                   p2 > 0 ? 1 : 0, p2 > 0 ? 0 : digit_shift(p1, 0), p2 > 0 ? digit_shift(p2, 0) : 0, n, tb.single,
+                   tb.sc, cond, use_cond ? 1 : 0);
         L += 1;
         cudaStream_t fs = st;
         cudaError_t e;

@@ -1,12 +1,12 @@
 """GPU: every sort plan of the octree build gives the same octree.
 
 A fresh context sorts both key words in full (16 passes of 8 bits). Later builds
-sort only the key bits that the last build's deepest split needed plus one octree
-level: the top bits of the first word (octree levels 1-21), or all of it and the
-top bits of the second (levels 22-42). A check for equal neighbours over those
-bits follows every planned sort, and the full sort runs on the device when the
-plan was short. Whatever the plan, accepted-node counts must equal the oracle's
-and the forces must not change."""
+sort only the key bits that the last build's deepest split needed: the top bits
+of the first word (octree levels 1-21), or all of it and the top bits of the
+second (levels 22-42). Runs of neighbours left equal over those bits are then
+sorted in place by their full keys (runs of at most 64), and a longer run makes
+the full sort run on the device. Whatever the plan, accepted-node counts must
+equal the oracle's and the forces must not change."""
 import numpy as np
 import pytest
 
@@ -23,8 +23,8 @@ def clustered_with_outliers(nb, n=5000):
 
 
 def planned_passes(split_bits):
-    """Passes of the plan that covers `split_bits` plus one octree level."""
-    bits = split_bits + 3
+    """Passes of the plan that covers `split_bits`."""
+    bits = split_bits
     if bits <= 63:
         return (bits + 7) // 8
     return 8 + (bits - 63 + 7) // 8 if bits <= 126 else 16
@@ -47,13 +47,13 @@ def test_sort_plans_agree(nb, orc, precision):
         st = e.stats()
         assert st["sort_passes"] == 16
         split = st["sort_split_bits"]
-        assert 3 <= split <= 63 - 3
+        assert 3 <= split <= 63 - 8
         # the second call sorts only the top bits of the first word
         a_s1, c_s1 = e.barnes_hut(spread, ms, counts=True)
-        assert e.stats()["sort_passes"] == planned_passes(split) < 8
+        assert e.stats()["sort_passes"] == planned_passes(split) < 8 and e.stats()["sort_tie_runs"] == 0
         assert np.array_equal(c_s1, rc_spread) and np.array_equal(a_s1, a_s)
-        # planned for the spread state, but this one needs the second word: the
-        # device runs the full sort after the planned one
+        # planned for the spread state, but this one needs the second word and the
+        # cluster is one run of thousands: the device runs the full sort after the planned one
         a_t, c_t = e.barnes_hut(tied, mt, counts=True)
         st = e.stats()
         assert st["sort_passes"] == planned_passes(split) + 16
@@ -73,13 +73,15 @@ def test_sort_plans_agree(nb, orc, precision):
         assert np.array_equal(a_s3, a_s)
 
 
-@pytest.mark.parametrize("single", [False, True])
-def test_plan_one_level_short(nb, orc, single):
-    """A state whose deepest split lies below the plan's extra level: the check
-    finds the equal neighbours and the full sort runs (FP64 and FLOAT builds)."""
+@pytest.mark.parametrize("single,offset", [(False, 1e-4), (False, 1e-7), (True, 1e-4)])
+def test_short_plan_runs_sorted_in_place(nb, orc, single, offset):
+    """A state whose deepest split lies below the plan's bits: the close pair is a
+    run of equal neighbours, sorted in place by its full keys (by the first word
+    at 1e-4, where the second word is not needed; by the second word, computed for
+    the run, at 1e-7). FP64 and FLOAT builds."""
     pos, _, mass = nb.generate(20000, gen_type=2, size=1024.0, seed=7)
     deeper = pos.copy()
-    deeper[1] = deeper[0] + np.array([1e-4, -2e-4, 1e-4])  # a pair much closer than any other
+    deeper[1] = deeper[0] + np.array([1.0, -2.0, 1.0]) * offset  # a pair much closer than any other
     dt = 4 if single else 8
     _, rc = orc.forces(deeper, mass, 0.5, single=single)
     with nb.Engine(datatype_bytes=dt) as e:
@@ -88,12 +90,16 @@ def test_plan_one_level_short(nb, orc, single):
         split = e.stats()["sort_split_bits"]
         acc, cnt = e.barnes_hut(deeper, mass, counts=True)
         st = e.stats()
-        assert st["sort_split_bits"] > split + 3
-        assert st["sort_passes"] == planned_passes(split) + 16
+        assert st["sort_split_bits"] > split
+        assert st["sort_passes"] == planned_passes(split)  # no full sort
+        assert st["sort_tie_runs"] >= 1
         assert np.array_equal(cnt, rc)
+        acc2, cnt2 = e.barnes_hut(deeper, mass, counts=True)  # the grown plan: no runs
+        assert e.stats()["sort_tie_runs"] == 0
     with nb.Engine(datatype_bytes=dt) as fresh:
         acc_full, cnt_full = fresh.barnes_hut(deeper, mass, counts=True)
-    assert np.array_equal(acc, acc_full) and np.array_equal(cnt, cnt_full)
+    for a, c in ((acc, cnt), (acc2, cnt2)):
+        assert np.array_equal(a, acc_full) and np.array_equal(c, cnt_full)
 
 
 def test_graph_replay_across_plans(nb):
