@@ -1041,7 +1041,7 @@ cudaError_t launch_walk(const WalkArgs &a, bool fp64, const WalkLaunch &l, cudaS
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
-    cfg.numAttrs = (st == nullptr || st == cudaStreamLegacy) ? 0 : 1;  // the legacy default stream: plain launch
+    cfg.numAttrs = 1;
     return cudaLaunchKernelExC(&cfg, k, params);
 }
 

@@ -168,9 +168,9 @@ def test_step_host_on_a_caller_stream(nb):
 
 @pytest.mark.parametrize("stream", [0, 2])  # the legacy default stream, the per-thread default stream
 def test_steps_on_the_default_streams(nb, stream):
-    """On the default streams the chained launches and the captured graphs give
-    the same steps as the engine's own stream (the legacy stream is launched
-    without the programmatic-dependency attribute and not captured)."""
+    """On the default streams the chained launches (and, on the per-thread
+    stream, the captured graphs; the legacy stream is not captured) give the same
+    steps as the engine's own stream."""
     import ctypes
     pos, vel, mass = nb.generate(30000, gen_type=2, size=1024.0, seed=3)
     with nb.Engine(adaptive=1) as e, nb.Engine(adaptive=1) as ref:
