@@ -232,7 +232,10 @@ def run_ours(args) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
     nbbuild.build()
-    stream = torch.cuda.current_stream()
+    # a stream of its own (the legacy default stream cannot be captured, so the
+    # engine would launch every kernel of every step one by one)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     g = nb.gen_params(gen_type=2, size=1024.0, r_sphere=100.0, rotation_magnitude=0.1, seed=0xDEADBEEF + rank)
     pos0, vel0, mass = nb.generate(args.n, g)
     adaptive = dict(adaptive=1, min_adaptive_dt=0.00333, max_pos_change=3.0, max_vel_change=3.0)

@@ -115,6 +115,9 @@ struct nbody_ctx {
     std::vector<unsigned char> step_key, adj_key;
     cudaGraphExec_t step_exec = nullptr;
     unsigned step_launches = 0;
+    unsigned step_cond_launches = 0;  // of those, the kernels of the full sort's conditional node
+    unsigned capture_cond_launches = 0;
+    unsigned replayed_cond_launches = 0;  // of the last replayed step, added if its full sort ran
     std::vector<cudaGraphExec_t> rec_exec, adj_exec;
     std::vector<unsigned> rec_launches, adj_launches;
     // image rendering buffers (grown on demand)
@@ -254,6 +257,8 @@ int check_status(nbody_ctx *c) {
     s.walk_decisions = h.walk_decisions;
     s.walk_list = h.walk_list;
     s.walk_near = h.walk_near;
+    if (h.word_ties) c->launches += c->replayed_cond_launches;  // the replayed step ran its full sort
+    c->replayed_cond_launches = 0;
     s.kernel_launches = c->launches;
     {
         const WalkLaunch &w = c->p.precision == NBODY_PRECISION_FP64 ? c->wl_fp64 : c->wl_mixed;
@@ -301,6 +306,7 @@ void tree_inputs(nbody_ctx *c, uint32_t n, bool want_vmax) {
     tb.sort_p2 = c->sort_p2;
     tb.sort_checked = 1;
     tb.cond_stream = c->cond_stream;
+    tb.cond_launches = &c->capture_cond_launches;
 }
 
 void ev(nbody_ctx *c, int k) {
@@ -674,13 +680,17 @@ int run_steps(nbody_ctx *c, uint32_t nsteps) {
         if (!c->step_exec || key != c->step_key) {
             drop_graph(c->step_exec);
             c->step_key.clear();
+            c->capture_cond_launches = 0;
             if (capture(c, &c->step_exec, &c->step_launches, [&] { return one_step(c); })) c->step_key = key;
+            c->step_cond_launches = c->capture_cond_launches;
         }
         if (c->step_exec) {
+            // the conditional node's kernels are counted when a replay ran them (check_status)
             for (uint32_t s = 0; s < nsteps; s++) {
                 NB_CUDA(cudaGraphLaunch(c->step_exec, c->stream));
-                c->launches += c->step_launches;
+                c->launches += c->step_launches - c->step_cond_launches;
             }
+            c->replayed_cond_launches = c->step_cond_launches;
             return NBODY_OK;
         }
     }

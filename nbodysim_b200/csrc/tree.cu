@@ -852,6 +852,7 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
             fs = tb.cond_stream;
         }
         // the full sort by (k1, k2): 8 passes on k2, the gather of k1, 8 passes on k1
+        const unsigned body_first = L;
         if (p2 == 0) {
             launch_pdl(k_keys_second, dim3(blocks_for(n, 256)), dim3(256), 0, fs, tb.pos, n, tb.sc, tb.key2, tb.single, ties);
             L += 1;
@@ -868,6 +869,7 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
         if (use_cond) {
             cudaGraph_t body = nullptr;
             if ((e = cudaStreamEndCapture(fs, &body)) != cudaSuccess) return e;
+            if (tb.cond_launches) *tb.cond_launches += L - body_first;
         }
     }
     if (multi) {

@@ -23,6 +23,8 @@ struct TreeBuild {
     int sort_p1, sort_p2, sort_checked;
     cudaStream_t cond_stream;   // captures the full sort into a conditional graph node (used only
                                 // while the build stream is being captured; null: never)
+    unsigned *cond_launches;    // non-null: adds the kernels put in that conditional node (they
+                                // run only when the planned sort left a long run)
     int single;                 // the reference's FLOAT build: positions and masses are read as
                                 // floats; root cube, child centres, node masses and centres of
                                 // mass are computed in float arithmetic
