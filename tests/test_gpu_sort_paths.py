@@ -119,3 +119,26 @@ def test_graph_replay_across_plans(nb):
             e.step(3)
             out.append(e.get_particles())
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def test_short_plan_runs_in_the_second_word(nb, orc):
+    """A plan that sorts all of the first word and the top bits of the second: a
+    pair closer than its bits resolve is a run sorted in place by the gathered
+    second words."""
+    tied, mt = clustered_with_outliers(nb)
+    deeper = tied.copy()
+    deeper[3] = deeper[2] + np.array([1.0, 1.0, -1.0]) * 1e-5  # ~40 levels below a 2e7 root: within the second word
+    _, rc = orc.forces(deeper, mt, 0.5)
+    with nb.Engine() as e:
+        e.barnes_hut(tied, mt)
+        e.barnes_hut(tied, mt)
+        split = e.stats()["sort_split_bits"]
+        assert 8 < planned_passes(split) < 16
+        acc, cnt = e.barnes_hut(deeper, mt, counts=True)
+        st = e.stats()
+        assert split < st["sort_split_bits"] <= 126 and st["sort_tie_runs"] >= 1
+        assert st["sort_passes"] == planned_passes(split)
+        assert np.array_equal(cnt, rc)
+    with nb.Engine() as fresh:
+        acc_full, cnt_full = fresh.barnes_hut(deeper, mt, counts=True)
+    assert np.array_equal(acc, acc_full) and np.array_equal(cnt, cnt_full)
