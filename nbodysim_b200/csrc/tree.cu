@@ -654,14 +654,11 @@ __device__ inline float div_rn(float a, float b) { return __fdiv_rn(a, b); }
 
 // One node's mass and centre of mass from its children, in the arithmetic of
 // T (double, or float for the reference's FLOAT build).
+// The node's child list comes in as c0, c1 (its eight slots).
 template <typename T>
-__device__ inline double4 node_com(const double4 *__restrict__ body, const int32_t *__restrict__ ochild,
-                                   const int32_t *__restrict__ ometa, const double4 *onode, int p, int L, int nch) {
+__device__ inline double4 node_com(const double4 *__restrict__ body, int4 c0, int4 c1,
+                                   const int32_t *__restrict__ ometa, const double4 *onode, int L, int nch) {
     T m = 0, sx = 0, sy = 0, sz = 0;
-    // the child list in two 16-byte loads, so that each child's values are one load away
-    const int4 *cp = reinterpret_cast<const int4 *>(ochild + 8 * (size_t)p);
-    const int4 c0 = cp[0];
-    const int4 c1 = nch > 4 ? cp[1] : make_int4(0, 0, 0, 0);
     for (int k = 0; k < nch; k++) {
         const int4 h = k < 4 ? c0 : c1;  // selects, not an indexed array (which would live in local memory)
         const int c = (k & 2) ? ((k & 1) ? h.w : h.z) : ((k & 1) ? h.y : h.x);
@@ -723,8 +720,14 @@ __global__ void __launch_bounds__(256, 4)
             atomicOr(&sc->status, kStatusCapacity);
             return;
         }
+        // The node's structure is final (the collapse wrote it): its metadata, child
+        // list and parent load before the arrival count, so that after it only the
+        // children's values remain to be read.
         const int32_t meta = ometa[p];
         const int nch = meta_nchild(meta);
+        const int4 *cp = reinterpret_cast<const int4 *>(ochild + 8 * (size_t)p);
+        const int4 c0 = __ldg(cp), c1 = __ldg(cp + 1);
+        const int up = oparent[p];
         if (hops > 0) {
             // One acquire-release count: it publishes the node this thread wrote on
             // the previous hop, and the last node child to arrive sees every
@@ -736,11 +739,11 @@ __global__ void __launch_bounds__(256, 4)
         // The reference sums the masses, then the mass-weighted centres, each in
         // child order; both sums run here in one pass over the children.
         const int L = meta_level(meta);
-        const double4 out = node_com<T>(body, ochild, ometa, onode, p, L, nch);
+        const double4 out = node_com<T>(body, c0, c1, ometa, onode, L, nch);
         double2 *q = reinterpret_cast<double2 *>(&onode[p]);
         __stcg(q, make_double2(out.x, out.y));
         __stcg(q + 1, make_double2(out.z, out.w));
-        p = oparent[p];
+        p = up;
     }
 }
 
