@@ -86,6 +86,39 @@ def test_oracle_equals_reference_live(orc, ref, oracle_mod, gt, n, theta, damp):
     assert np.array_equal(a_ref, a_or)
 
 
+@pytest.mark.parametrize("gt", [0, 1, 2])
+def test_threaded_reference_equals_serial_build(ref, oracle_mod, gt):
+    """With threads > 1 the reference builds its tree with gen_root_threaded
+    (src/main.cpp:837-886): all 8 root children pre-allocated, each filled by
+    its own thread through the closed inside() test (src/octree.cpp:320-336).
+    On the seeded cube, sphere and shell that build gives the serial build's
+    accelerations bit for bit, so the multi-threaded reference timings walk
+    the same tree this library follows."""
+    g = oracle_mod.GenParams(gen_type=gt, size=1024.0, r_sphere=100.0, rotation_magnitude=0.1)
+    p, _, m = ref.generate(g, 20000)
+    for theta in (0.5, 2.0):
+        a1, _ = ref.forces(p, m, theta, threads=1)
+        a8, _ = ref.forces(p, m, theta, threads=8)
+        assert np.array_equal(a1, a8)
+
+
+def test_threaded_reference_inserts_split_plane_particles_twice(ref):
+    """The one place the two builds part: a particle exactly on a root split
+    plane passes inside() for both neighbouring root children, so the threaded
+    build holds it twice and every other particle feels it twice."""
+    p = np.array([[-10.0, -3.0, 2.0], [0.0, 1.0, -1.0], [10.0, 4.0, -5.0], [5.0, -6.0, 7.0]])
+    m = np.array([1e10, 2e10, 3e10, 4e10])  # root centre x = 0: particle 1 lies on the x split plane
+    a1, _ = ref.forces(p, m, 0.5, threads=1)
+    a8, _ = ref.forces(p, m, 0.5, threads=8)
+    # it skips both of its own leaves (the sum order differs, so to rounding)
+    assert np.allclose(a1[1], a8[1], rtol=1e-14, atol=0)
+    G = 6.67384e-11
+    for i in (0, 2, 3):  # the others take it twice
+        d = p[1] - p[i]
+        extra = G * m[1] * d / np.linalg.norm(d) ** 3
+        assert np.allclose(a8[i] - a1[i], extra, rtol=1e-9, atol=0)
+
+
 def test_oracle_frames_equal_reference_live(orc, ref, oracle_mod):
     p, v, m = ref.generate(oracle_mod.GenParams(gen_type=1), 800)
     _, _, f1 = ref.run_frames(p, v, m, 4, keep_frames=True)
