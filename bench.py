@@ -291,7 +291,7 @@ def run_ours(args) -> None:
         ph["walk"].append(s_["ms_walk"]); ph["update"].append(s_["ms_update"])
         ph["inter"].append(s_["interactions"])
     eng.set_timing(False)
-    sort_plan = {"passes": s_["sort_passes"], "split_bits": s_["sort_split_bits"]}
+    sort_plan = {"passes": s_["sort_passes"], "split_bits": s_["sort_split_bits"], "tie_runs": s_["sort_tie_runs"]}
     walk_ms = float(np.mean(ph["walk"]))
     walk_inter = float(np.mean(ph["inter"]))
 

@@ -38,9 +38,10 @@
 extern "C" {
 #endif
 
-#define NBODY_ABI_VERSION 6  /* 2: nbody_params.autotune, nbody_stats walk fields; 3: merging;
+#define NBODY_ABI_VERSION 7  /* 2: nbody_params.autotune, nbody_stats walk fields; 3: merging;
                                 4: nbody_params.datatype_bytes; 5: nbody_stats sort fields;
-                                6: nbody_stats.sort_tie_runs, nbody_set_walk_stats */
+                                6: nbody_stats.sort_tie_runs, nbody_set_walk_stats;
+                                7: nbody_stats.sort_next_passes */
 
 /* ---- status codes ---------------------------------------------------- */
 #define NBODY_OK 0
@@ -178,9 +179,14 @@ typedef struct nbody_stats {
                                   plus the full sort's 16 when the plan left a run of more than
                                   64 equal neighbours */
     uint32_t sort_split_bits;  /* key bits (3 per octree level) that separate every pair of
-                                  Morton neighbours in the last build; the next plan covers them */
+                                  Morton neighbours in the last build */
     uint32_t sort_tie_runs;    /* runs of neighbours equal over the planned bits (at most 64 each)
                                   that the last build sorted in place */
+    uint32_t sort_next_passes; /* passes the next build plans: the fewest that leave at most
+                                  max(64, n / 16) pairs of the last build's neighbours tied (sorted
+                                  in place as runs); for 8 calls after a build ran the full sort,
+                                  the ones that cover sort_split_bits; 16 when a pair needs a third
+                                  key word. A plan shrinks by two passes or more at a time. */
 } nbody_stats;
 int nbody_get_stats(nbody_ctx *ctx, nbody_stats *out);
 /* Time phases with CUDA events on the context stream (default off; timed calls

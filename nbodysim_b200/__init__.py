@@ -75,6 +75,7 @@ class Stats(C.Structure):
         ("ms_tree", C.c_float), ("ms_com", C.c_float), ("ms_walk", C.c_float), ("ms_update", C.c_float),
         ("merged_min_size", C.c_uint64), ("merged_collisions", C.c_uint64), ("collision_pairs", C.c_uint64),
         ("sort_passes", C.c_uint32), ("sort_split_bits", C.c_uint32), ("sort_tie_runs", C.c_uint32),
+        ("sort_next_passes", C.c_uint32),
     ]
 
     def as_dict(self) -> dict:

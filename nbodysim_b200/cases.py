@@ -41,7 +41,7 @@ def walk_case(args) -> None:
             e.barnes_hut(pos, mass, theta=args.theta)
         s = e.stats()
     print({k: s[k] for k in ("interactions", "walk_list", "walk_near", "walk_tiles", "walk_decisions",
-                             "tree_nodes", "tree_depth", "sort_passes", "sort_split_bits")})
+                             "tree_nodes", "tree_depth", "sort_passes", "sort_split_bits", "sort_tie_runs")})
 
 
 def adjoint_case(args) -> None:

@@ -105,10 +105,12 @@ struct nbody_ctx {
     int32_t *sys_root_node = nullptr;
     bool single_pass = false;  // nbody_barnes_hut: one system regardless of the layout
     // Sort plan of the next tree build (TreeBuild::sort_p1, sort_p2): the full
-    // two-word sort until a build has measured its deepest split, then only the
-    // key bits that split needs plus one octree level. The build checks the plan
-    // itself and falls back to the full sort on the device when it is short.
+    // two-word sort until a build has measured its pairs of neighbours, then the
+    // passes next_sort_plan picks from them. The build sorts the runs of
+    // neighbours the plan leaves tied in place, and falls back to the full sort
+    // on the device when a run is too long for that.
     int sort_p1 = 8, sort_p2 = 8;
+    int sort_cooldown = 0;  // calls left whose plan follows the deepest split
     // CUDA graphs: one captured step replayed per step; per-offset graphs for the
     // adjoint's recompute and reverse steps. Rebuilt when their key changes.
     bool use_graphs = true;
@@ -226,21 +228,37 @@ int reserve(nbody_ctx *c, uint32_t n) {
     return NBODY_OK;
 }
 
-// The next build's sort plan from the last build's deepest split (the key bits
-// that separate every pair of neighbours), in whole 8-bit passes: the top bits
-// of the first word, or all of it and the top bits of the second. A plan
-// shrinks only by two passes or more, so that small changes do not rebuild
-// captured graphs; it grows at once after a build whose plan was short (it
-// sorted runs of equal neighbours in place, or ran the full sort). No split
-// measured: keep the plan.
-void next_sort_plan(nbody_ctx *c, uint32_t need_bits, bool short_plan) {
-    if (need_bits == 0) return;
-    const uint32_t bits = need_bits;
-    int p1 = 8, p2 = 8;
-    if (bits <= 63) { p1 = (int)(bits + 7) / 8; p2 = 0; }
-    else if (bits <= 126) { p2 = (int)(bits - 63 + 7) / 8; }
-    const int cur = c->sort_p1 + c->sort_p2, want = p1 + p2;
-    if (short_plan || want > cur || cur - want >= 2) {
+// The next build's sort plan, in whole 8-bit passes: the top bits of the first
+// key word, or all of it and the top bits of the second. The deepest split of
+// the last build (the key bits that separate every pair of neighbours) gives
+// the plan that leaves no ties; the plan taken is the fewest passes that leave
+// at most max(64, n / kTieShare) pairs of neighbours tied, which the build sorts
+// in place as short runs. After a build whose runs were too long for that (it
+// ran the full sort), the deepest split sets the plan for kPlanCooldown calls;
+// a split beyond two key words keeps the full sort. A plan shrinks only by two
+// passes or more, so that small changes do not rebuild captured graphs; it
+// grows at once. No split measured: keep the plan.
+constexpr uint32_t kTieShare = 16;
+constexpr int kPlanCooldown = 8;
+
+void next_sort_plan(nbody_ctx *c, const DevScalars &h) {
+    if (h.max_prefix_bits == 0) return;
+    const int deepest = std::min(passes_for_bits(h.max_prefix_bits), 16);
+    if (h.word_ties) c->sort_cooldown = kPlanCooldown;
+    int want = deepest;
+    if (deepest < 16 && c->sort_cooldown == 0) {
+        const uint64_t tol = std::max<uint64_t>(64, c->n / kTieShare);
+        uint64_t tied = 0;  // pairs that a plan of want - 1 passes leaves tied
+        while (want > 1) {
+            tied += h.pair_passes[want];
+            if (tied > tol) break;
+            want--;
+        }
+    }
+    if (c->sort_cooldown > 0) c->sort_cooldown--;
+    const int p1 = std::min(want, 8), p2 = want - p1;
+    const int cur = c->sort_p1 + c->sort_p2;
+    if (h.word_ties || want > cur || cur - want >= 2) {
         c->sort_p1 = p1;
         c->sort_p2 = p2;
     }
@@ -278,7 +296,8 @@ int check_status(nbody_ctx *c) {
     s.sort_passes = c->nsys > 1 ? 18u : (uint32_t)(c->sort_p1 + c->sort_p2) + (h.word_ties ? 16u : 0u);
     s.sort_split_bits = h.max_prefix_bits;
     s.sort_tie_runs = h.tie_runs;
-    next_sort_plan(c, h.max_prefix_bits, h.word_ties != 0 || h.tie_runs != 0);
+    next_sort_plan(c, h);
+    s.sort_next_passes = c->nsys > 1 ? 18u : (uint32_t)(c->sort_p1 + c->sort_p2);
     if (c->timing) {
         float ms[4] = {0, 0, 0, 0};
         for (int k = 0; k < 4; k++) cudaEventElapsedTime(&ms[k], c->ev[k], c->ev[k + 1]);

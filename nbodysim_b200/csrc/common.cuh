@@ -63,6 +63,14 @@ enum : uint32_t {
     kStatusSortStall = 1u << 4,  // a radix-sort look-back gave up waiting (never expected)
 };
 
+// Pairs of neighbouring keys are binned by the sort passes that separate them:
+// 1-8 passes cover the first 63-bit key word, 9-16 also the second; bin 17 is a
+// pair equal over both words.
+constexpr int kPassBins = 18;
+__host__ __device__ inline int passes_for_bits(uint32_t bits) {
+    return bits <= 63 ? (int)(bits + 7) / 8 : bits <= 126 ? 8 + (int)(bits - 63 + 7) / 8 : kPassBins - 1;
+}
+
 struct DevScalars {
     double root_center[3];
     double root_side;
@@ -87,6 +95,8 @@ struct DevScalars {
     uint32_t tie_runs;        // short runs of equal neighbours the last build sorted in place
     uint32_t max_prefix_bits; // deepest split of the last build: key bits that separate every
                               // pair of neighbours (the longest common prefix + 1)
+    uint32_t pair_passes[kPassBins];  // the last build's pairs of neighbours by the 8-bit sort passes
+                                      // that separate them (kPassBins - 1: more than two key words)
     unsigned long long max_acc_bits;  // max |a| (non-negative double as ordered bits)
     unsigned long long max_vel_bits;  // max |v|
     double dt_used;

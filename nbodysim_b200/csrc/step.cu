@@ -124,6 +124,7 @@ __global__ void k_reset_pass(DevScalars *sc) {
     sc->word_ties = 0;
     sc->tie_runs = 0;
     sc->max_prefix_bits = 0;
+    for (int k = 0; k < kPassBins; k++) sc->pair_passes[k] = 0;
     sc->max_acc_bits = 0;
     sc->max_vel_bits = 0;
 }

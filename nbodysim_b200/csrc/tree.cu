@@ -271,15 +271,50 @@ __global__ void k_fix_ties(uint64_t *__restrict__ k1_sorted, uint64_t *__restric
     }
     atomicAdd(&sc->tie_runs, 1u);
     if (!have_k2) {
-        const double root[4] = {sc->root_center[0], sc->root_center[1], sc->root_center[2], sc->root_side};
-        for (uint32_t q = j; q <= e; q++) {
-            const size_t u = 3 * (size_t)idx[q];
-            const double p[3] = {pos[u], pos[u + 1], pos[u + 2]};
-            uint64_t w[2];
-            if (single) descend_words<float>(p, root, 2, w);
-            else descend_words<double>(p, root, 2, w);
-            k2_sorted[q] = w[1];
+        // The plan sorted top bits of the first word only: the run is sorted by its
+        // first words, and only a stretch of equal first words needs the second
+        // word, computed for it here (stable sorts both, as the full sort is).
+        for (uint32_t q = j + 1; q <= e; q++) {
+            const uint64_t a1 = k1_sorted[q];
+            const uint32_t ai = idx[q];
+            uint32_t p = q;
+            while (p > j && k1_sorted[p - 1] > a1) {
+                k1_sorted[p] = k1_sorted[p - 1];
+                idx[p] = idx[p - 1];
+                p--;
+            }
+            k1_sorted[p] = a1;
+            idx[p] = ai;
         }
+        const double root[4] = {sc->root_center[0], sc->root_center[1], sc->root_center[2], sc->root_side};
+        for (uint32_t a = j; a < e;) {
+            uint32_t b = a;
+            while (b < e && k1_sorted[b + 1] == k1_sorted[a]) b++;
+            if (b > a) {
+                for (uint32_t q = a; q <= b; q++) {
+                    const size_t u = 3 * (size_t)idx[q];
+                    const double p[3] = {pos[u], pos[u + 1], pos[u + 2]};
+                    uint64_t w[2];
+                    if (single) descend_words<float>(p, root, 2, w);
+                    else descend_words<double>(p, root, 2, w);
+                    k2_sorted[q] = w[1];
+                }
+                for (uint32_t q = a + 1; q <= b; q++) {
+                    const uint64_t a2 = k2_sorted[q];
+                    const uint32_t ai = idx[q];
+                    uint32_t p = q;
+                    while (p > a && k2_sorted[p - 1] > a2) {
+                        k2_sorted[p] = k2_sorted[p - 1];
+                        idx[p] = idx[p - 1];
+                        p--;
+                    }
+                    k2_sorted[p] = a2;
+                    idx[p] = ai;
+                }
+            }
+            a = b + 1;
+        }
+        return;
     }
     for (uint32_t q = j + 1; q <= e; q++) {
         const uint64_t a1 = k1_sorted[q], a2 = k2_sorted[q];
@@ -502,7 +537,8 @@ __device__ inline int level_of(int delta) { return min(delta / 3, kMaxLevels); }
 
 __global__ void k_radix_tree(KeyView kv, int32_t *__restrict__ bleft, int32_t *__restrict__ bright,
                              int32_t *__restrict__ bparent, int32_t *__restrict__ leaf_bparent,
-                             int32_t *__restrict__ bdelta, uint32_t *max_prefix_bits) {
+                             int32_t *__restrict__ bdelta, uint32_t *max_prefix_bits, uint32_t *pair_passes) {
+    __shared__ uint32_t hist[kPassBins];
     griddep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = kv.n;
@@ -510,6 +546,18 @@ __global__ void k_radix_tree(KeyView kv, int32_t *__restrict__ bleft, int32_t *_
     const int dn = i < n - 1 ? kv.delta(i, i + 1) : -1;
     const int wmax = __reduce_max_sync(0xffffffffu, dn);
     if ((threadIdx.x & 31) == 0 && wmax >= 0) atomicMax(max_prefix_bits, (uint32_t)wmax + 1u);
+    // the pairs by the sort passes that separate them (the next build's plan):
+    // per warp one shared-memory add per distinct pass count, per block one
+    // global add per nonzero bin
+    if (threadIdx.x < kPassBins) hist[threadIdx.x] = 0u;
+    __syncthreads();
+    {
+        const int bin = dn >= 0 ? passes_for_bits((uint32_t)dn + 1u) : -1;
+        const uint32_t same = __match_any_sync(0xffffffffu, bin);
+        if (bin >= 0 && (threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&hist[bin], (uint32_t)__popc(same));
+    }
+    __syncthreads();
+    if (threadIdx.x < kPassBins && hist[threadIdx.x]) atomicAdd(&pair_passes[threadIdx.x], hist[threadIdx.x]);
     if (i >= n - 1) return;
     // With several systems, the internal nodes of the system [s, e) are s..e-2:
     // the last particle of a system indexes no internal node.
@@ -898,7 +946,7 @@ cudaError_t build_octree(const TreeBuild &tb, cudaStream_t st, unsigned *launche
     KeyView kv{tb.key_b, tb.key_a, tb.key3, (int)n, sys_sorted};
     const uint32_t m = n - 1;
     launch_pdl(k_radix_tree, dim3(blocks_for(m, 256)), dim3(256), 0, st, kv, tb.bleft, tb.bright, tb.bparent, tb.leaf_bparent,
-                                                      tb.bdelta, &tb.sc->max_prefix_bits);
+                                                      tb.bdelta, &tb.sc->max_prefix_bits, tb.sc->pair_passes);
     launch_pdl(k_head_flags, dim3(blocks_for(n, 256)), dim3(256), 0, st, tb.bparent, tb.bdelta, m, tb.head_flag,
                tb.head_id, tb.oparent, tb.leaf_oparent, tb.ocount);
     L += 3 + scan_exclusive(tb.head_id, m, tb.scan_tmp, &tb.sc->n_onodes, st);

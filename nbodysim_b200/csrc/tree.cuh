@@ -16,10 +16,13 @@ struct TreeBuild {
     // Sort plan (single system). sort_p2 passes sort the top 8 sort_p2 bits of
     // the second key word (levels 22-42; 0: none), then sort_p1 passes the top
     // 8 sort_p1 bits of the first word (levels 1-21); 8 passes take a whole
-    // word. With sort_checked, a check for equal neighbours over those bits
-    // follows and the full two-word sort runs on the device only when it finds
-    // one (sc->word_ties), so a plan that covers too few bits costs time, not
-    // results. Several systems always take the full sort.
+    // word. With sort_checked, runs of neighbours equal over those bits are
+    // sorted in place by their full keys (sc->tie_runs), and the full two-word
+    // sort runs on the device only when a run is longer than 64 (sc->word_ties),
+    // so a plan that covers too few bits costs time, not results. The build
+    // bins the pairs of neighbours by the passes that separate them
+    // (sc->pair_passes) for the next plan. Several systems always take the full
+    // sort.
     int sort_p1, sort_p2, sort_checked;
     cudaStream_t cond_stream;   // captures the full sort into a conditional graph node (used only
                                 // while the build stream is being captured; null: never)

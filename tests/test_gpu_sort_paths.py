@@ -1,11 +1,13 @@
 """GPU: every sort plan of the octree build gives the same octree.
 
 A fresh context sorts both key words in full (16 passes of 8 bits). Later builds
-sort only the key bits that the last build's deepest split needed: the top bits
-of the first word (octree levels 1-21), or all of it and the top bits of the
-second (levels 22-42). Runs of neighbours left equal over those bits are then
-sorted in place by their full keys (runs of at most 64), and a longer run makes
-the full sort run on the device. Whatever the plan, accepted-node counts must
+sort only top key bits: the first word's (octree levels 1-21), or all of it and
+the second word's (levels 22-42). The plan is the fewest passes that leave at
+most max(64, n / 16) pairs of the last build's neighbours tied. Runs of
+neighbours left equal over the planned bits are sorted in place by their full
+keys (runs of at most 64); a longer run makes the full sort run on the device,
+after which the plans cover the deepest split (the key bits that separate every
+pair of neighbours) for 8 calls. Whatever the plan, accepted-node counts must
 equal the oracle's and the forces must not change."""
 import numpy as np
 import pytest
@@ -48,19 +50,24 @@ def test_sort_plans_agree(nb, orc, precision):
         assert st["sort_passes"] == 16
         split = st["sort_split_bits"]
         assert 3 <= split <= 63 - 8
-        # the second call sorts only the top bits of the first word
+        # the second call sorts fewer top bits of the first word than the deepest
+        # split needs, and sorts the runs they leave in place
+        plan = st["sort_next_passes"]
         a_s1, c_s1 = e.barnes_hut(spread, ms, counts=True)
-        assert e.stats()["sort_passes"] == planned_passes(split) < 8 and e.stats()["sort_tie_runs"] == 0
+        st = e.stats()
+        assert st["sort_passes"] == plan < planned_passes(split) < 8 and st["sort_tie_runs"] > 0
+        assert st["sort_next_passes"] == plan
         assert np.array_equal(c_s1, rc_spread) and np.array_equal(a_s1, a_s)
         # planned for the spread state, but this one needs the second word and the
         # cluster is one run of thousands: the device runs the full sort after the planned one
         a_t, c_t = e.barnes_hut(tied, mt, counts=True)
         st = e.stats()
-        assert st["sort_passes"] == planned_passes(split) + 16
+        assert st["sort_passes"] == plan + 16
         assert np.array_equal(c_t, rc_tied)
         assert np.array_equal(a_t, a_tied_full)
-        # now all of the first word and the top bits of the second
+        # now, for a few calls, the deepest split: all of the first word and the top bits of the second
         split_t = st["sort_split_bits"]
+        assert st["sort_next_passes"] == planned_passes(split_t)
         a_t2, c_t2 = e.barnes_hut(tied, mt, counts=True)
         assert 8 < e.stats()["sort_passes"] == planned_passes(split_t) < 16
         assert np.array_equal(c_t2, rc_tied) and np.array_equal(a_t2, a_tied_full)
@@ -71,6 +78,13 @@ def test_sort_plans_agree(nb, orc, precision):
         a_s3, _ = e.barnes_hut(spread, ms, counts=True)
         assert e.stats()["sort_passes"] == planned_passes(split)
         assert np.array_equal(a_s3, a_s)
+        # once those calls are over, the fewer passes again
+        for _ in range(5):
+            a_s4, c_s4 = e.barnes_hut(spread, ms, counts=True)
+        assert e.stats()["sort_next_passes"] == plan
+        a_s4, c_s4 = e.barnes_hut(spread, ms, counts=True)
+        assert e.stats()["sort_passes"] == plan
+        assert np.array_equal(a_s4, a_s) and np.array_equal(c_s4, rc_spread)
 
 
 @pytest.mark.parametrize("single,offset", [(False, 1e-4), (False, 1e-7), (True, 1e-4)])
@@ -87,15 +101,16 @@ def test_short_plan_runs_sorted_in_place(nb, orc, single, offset):
     with nb.Engine(datatype_bytes=dt) as e:
         e.barnes_hut(pos, mass)
         e.barnes_hut(pos, mass)
-        split = e.stats()["sort_split_bits"]
+        st = e.stats()
+        split, plan = st["sort_split_bits"], st["sort_next_passes"]
         acc, cnt = e.barnes_hut(deeper, mass, counts=True)
         st = e.stats()
         assert st["sort_split_bits"] > split
-        assert st["sort_passes"] == planned_passes(split)  # no full sort
+        assert st["sort_passes"] == plan < 8  # no full sort
         assert st["sort_tie_runs"] >= 1
         assert np.array_equal(cnt, rc)
-        acc2, cnt2 = e.barnes_hut(deeper, mass, counts=True)  # the grown plan: no runs
-        assert e.stats()["sort_tie_runs"] == 0
+        acc2, cnt2 = e.barnes_hut(deeper, mass, counts=True)  # one more tied pair: still no full sort
+        assert e.stats()["sort_passes"] == st["sort_next_passes"] < 8
     with nb.Engine(datatype_bytes=dt) as fresh:
         acc_full, cnt_full = fresh.barnes_hut(deeper, mass, counts=True)
     for a, c in ((acc, cnt), (acc2, cnt2)):
@@ -132,12 +147,13 @@ def test_short_plan_runs_in_the_second_word(nb, orc):
     with nb.Engine() as e:
         e.barnes_hut(tied, mt)
         e.barnes_hut(tied, mt)
-        split = e.stats()["sort_split_bits"]
-        assert 8 < planned_passes(split) < 16
+        st = e.stats()
+        split, plan = st["sort_split_bits"], st["sort_next_passes"]
+        assert 8 < plan <= planned_passes(split) < 16
         acc, cnt = e.barnes_hut(deeper, mt, counts=True)
         st = e.stats()
         assert split < st["sort_split_bits"] <= 126 and st["sort_tie_runs"] >= 1
-        assert st["sort_passes"] == planned_passes(split)
+        assert st["sort_passes"] == plan
         assert np.array_equal(cnt, rc)
     with nb.Engine() as fresh:
         acc_full, cnt_full = fresh.barnes_hut(deeper, mt, counts=True)
