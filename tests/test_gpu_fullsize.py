@@ -96,3 +96,24 @@ def test_sphere_100k_every_particle(nb, eng, orc):
     ra, rc = orc.forces(pos, mass, 0.5)
     assert np.array_equal(cnt, rc), f"{np.count_nonzero(cnt != rc)} particles differ"
     assert np.percentile(rel(acc, ra), 99) <= P99_MIXED
+
+
+@pytest.mark.parametrize("state", ["initial", "evolved"])
+def test_planned_sort_with_runs_equals_full_sort(nb, states, state):
+    """The planned sort at the headline size: a fresh context sorts both key words
+    in full; the next pass sorts the plan's passes (4 on the initial shell, where
+    the deepest split needs 6), fewer than the deepest split needs, and thousands
+    of runs of tied neighbours in place. Forces and counts are bit-identical."""
+    pos, mass = states[state]
+    with nb.Engine() as e:
+        acc_full, cnt_full = e.barnes_hut(pos, mass, counts=True)
+        st = e.stats()
+        assert st["sort_passes"] == 16
+        plan = st["sort_next_passes"]
+        acc, cnt = e.barnes_hut(pos, mass, counts=True)
+        st = e.stats()
+    deepest = (st["sort_split_bits"] + 7) // 8 if st["sort_split_bits"] <= 63 else \
+        8 + (st["sort_split_bits"] - 63 + 7) // 8
+    assert st["sort_passes"] == plan < deepest
+    assert st["sort_tie_runs"] > 1000
+    assert np.array_equal(cnt, cnt_full) and np.array_equal(acc, acc_full)
