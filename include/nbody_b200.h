@@ -182,11 +182,13 @@ typedef struct nbody_stats {
                                   Morton neighbours in the last build */
     uint32_t sort_tie_runs;    /* runs of neighbours equal over the planned bits (at most 64 each)
                                   that the last build sorted in place */
-    uint32_t sort_next_passes; /* passes the next build plans: the fewest that leave at most
-                                  max(64, n / 16) pairs of the last build's neighbours tied (sorted
-                                  in place as runs); for 8 calls after a build ran the full sort,
-                                  the ones that cover sort_split_bits; 16 when a pair needs a third
-                                  key word. A plan shrinks by two passes or more at a time. */
+    uint32_t sort_next_passes; /* passes the next single step or force pass plans: the fewest that
+                                  leave at most max(64, n / 16) pairs of the last build's neighbours
+                                  tied (sorted in place as runs); for 8 calls after a build ran the
+                                  full sort, the ones that cover sort_split_bits; 16 when a pair
+                                  needs a third key word. A call of several steps plans the passes
+                                  that cover sort_split_bits. A plan shrinks by two passes or more
+                                  at a time. */
 } nbody_stats;
 int nbody_get_stats(nbody_ctx *ctx, nbody_stats *out);
 /* Time phases with CUDA events on the context stream (default off; timed calls

@@ -111,6 +111,10 @@ struct nbody_ctx {
     // on the device when a run is too long for that.
     int sort_p1 = 8, sort_p2 = 8;
     int sort_cooldown = 0;  // calls left whose plan follows the deepest split
+    // Calls of several steps replay one captured step whose plan cannot change
+    // while the state drifts: they sort by the deepest split (sort_deep_p1, p2).
+    int sort_deep_p1 = 8, sort_deep_p2 = 8;
+    bool multi_step_call = false;
     // CUDA graphs: one captured step replayed per step; per-offset graphs for the
     // adjoint's recompute and reverse steps. Rebuilt when their key changes.
     bool use_graphs = true;
@@ -231,13 +235,19 @@ int reserve(nbody_ctx *c, uint32_t n) {
 // The next build's sort plan, in whole 8-bit passes: the top bits of the first
 // key word, or all of it and the top bits of the second. The deepest split of
 // the last build (the key bits that separate every pair of neighbours) gives
-// the plan that leaves no ties; the plan taken is the fewest passes that leave
-// at most max(64, n / kTieShare) pairs of neighbours tied, which the build sorts
-// in place as short runs. After a build whose runs were too long for that (it
-// ran the full sort), the deepest split sets the plan for kPlanCooldown calls;
-// a split beyond two key words keeps the full sort. A plan shrinks only by two
-// passes or more, so that small changes do not rebuild captured graphs; it
-// grows at once. No split measured: keep the plan.
+// the plan that leaves no ties. A single step or force pass takes the fewest
+// passes that leave at most max(64, n / kTieShare) pairs of neighbours tied,
+// which the build sorts in place as short runs; after a build whose runs were
+// too long for that (it ran the full sort), the deepest split sets that plan
+// for kPlanCooldown calls. A call of several steps replays one captured step
+// while the state drifts, and ties that grow past a run of 64 would make every
+// later step run the full sort: it takes the deepest split (the 256-step
+// forward of the adjoint's sphere of 65,536: 239 ms with the fewer passes, 180
+// ms with the deepest split). A split beyond two key words keeps the full sort.
+// A plan shrinks only by two passes or more, so that small changes do not
+// rebuild captured graphs; it grows at once, and the deepest-split plan also
+// follows a build that sorted runs or ran the full sort. No split measured:
+// keep the plans.
 constexpr uint32_t kTieShare = 16;
 constexpr int kPlanCooldown = 8;
 
@@ -262,7 +272,21 @@ void next_sort_plan(nbody_ctx *c, const DevScalars &h) {
         c->sort_p1 = p1;
         c->sort_p2 = p2;
     }
+    const int cur_deep = c->sort_deep_p1 + c->sort_deep_p2;
+    if (h.word_ties || h.tie_runs || deepest > cur_deep || cur_deep - deepest >= 2) {
+        c->sort_deep_p1 = std::min(deepest, 8);
+        c->sort_deep_p2 = deepest - c->sort_deep_p1;
+    }
 }
+
+// Marks an API call of several steps for its duration (tree_inputs picks the
+// deepest-split sort plan).
+struct MultiStepCall {
+    nbody_ctx *c;
+    bool saved;
+    MultiStepCall(nbody_ctx *ctx, bool multi) : c(ctx), saved(ctx->multi_step_call) { c->multi_step_call = multi; }
+    ~MultiStepCall() { c->multi_step_call = saved; }
+};
 
 int check_status(nbody_ctx *c) {
     NB_CUDA(cudaStreamSynchronize(c->stream));
@@ -293,7 +317,8 @@ int check_status(nbody_ctx *c) {
     s.last_dt = h.dt_used;
     for (int k = 0; k < 3; k++) s.root_center[k] = h.root_center[k];
     s.root_side = h.root_side;
-    s.sort_passes = c->nsys > 1 ? 18u : (uint32_t)(c->sort_p1 + c->sort_p2) + (h.word_ties ? 16u : 0u);
+    const int used_plan = c->multi_step_call ? c->sort_deep_p1 + c->sort_deep_p2 : c->sort_p1 + c->sort_p2;
+    s.sort_passes = c->nsys > 1 ? 18u : (uint32_t)used_plan + (h.word_ties ? 16u : 0u);
     s.sort_split_bits = h.max_prefix_bits;
     s.sort_tie_runs = h.tie_runs;
     next_sort_plan(c, h);
@@ -321,8 +346,8 @@ void tree_inputs(nbody_ctx *c, uint32_t n, bool want_vmax) {
     tb.vel_for_max = want_vmax ? c->vel : nullptr;
     tb.sc = c->sc;
     tb.single = single(c) ? 1 : 0;
-    tb.sort_p1 = c->sort_p1;
-    tb.sort_p2 = c->sort_p2;
+    tb.sort_p1 = c->multi_step_call ? c->sort_deep_p1 : c->sort_p1;
+    tb.sort_p2 = c->multi_step_call ? c->sort_deep_p2 : c->sort_p2;
     tb.sort_checked = 1;
     tb.cond_stream = c->cond_stream;
     tb.cond_launches = &c->capture_cond_launches;
@@ -467,7 +492,8 @@ std::vector<unsigned char> graph_key(nbody_ctx *c, uint32_t extra) {
     } k;
     std::memset(&k, 0, sizeof k);
     k.n = c->n; k.nsys = c->nsys; k.ngroups = c->ngroups; k.extra = extra;
-    k.sort_p1 = c->sort_p1; k.sort_p2 = c->sort_p2; k.walk_stats = c->walk_stats;
+    k.sort_p1 = c->multi_step_call ? c->sort_deep_p1 : c->sort_p1;
+    k.sort_p2 = c->multi_step_call ? c->sort_deep_p2 : c->sort_p2; k.walk_stats = c->walk_stats;
     k.arena = c->arena; k.adj = c->adj_arena; k.sys = c->sys_arena; k.stream = (void *)c->stream;
     k.p = c->p; k.wm = c->wl_mixed; k.wf = c->wl_fp64;
     const unsigned char *b = (const unsigned char *)&k;
@@ -1213,6 +1239,7 @@ int nbody_step(nbody_ctx *c, uint32_t nsteps) {
         return fail(NBODY_ERR_INVALID, "collisions and min_node_size need a single system%s");
     c->merged_min_size = c->merged_collisions = c->collision_pairs = 0;
     if (c->n == 0 || nsteps == 0) return NBODY_OK;
+    MultiStepCall scope(c, nsteps > 1);
     int rc = begin_call(c);
     if (rc) return rc;
     if ((rc = maybe_autotune(c))) return rc;
@@ -1229,6 +1256,7 @@ int nbody_step_host(nbody_ctx *c, uint32_t n, double *pos, double *vel, const do
     if (merging(c))
         return fail(NBODY_ERR_INVALID, "merging changes n: use nbody_set_particles, nbody_step, nbody_get_particles%s");
     if (n == 0) return NBODY_OK;
+    MultiStepCall scope(c, nsteps > 1);
     int rc;
     if (n >= kOverlapMin && nsteps > 0) {
         // Positions first: the root cube, keys and sort need nothing else. The
@@ -1376,6 +1404,7 @@ int nbody_forward_checkpointed(nbody_ctx *c, uint32_t nsteps, uint32_t every) {
     if (single(c)) return fail(NBODY_ERR_INVALID, "the adjoint needs datatype_bytes 8%s");
     c->have_fwd = false;
     if (nsteps == 0 || c->n == 0) return NBODY_OK;
+    MultiStepCall scope(c, nsteps > 1);
     if (every == 0) {
         every = 1;
         while ((uint64_t)every * every < nsteps) every++;
@@ -1415,6 +1444,7 @@ int nbody_backward(nbody_ctx *c, const double *dL_dpos, const double *dL_dvel, d
     const size_t N3 = 3 * (size_t)n;
     const bool fp64 = c->p.precision == NBODY_PRECISION_FP64;
     if (c->p.dt != c->fwd_dt) return fail(NBODY_ERR_STATE, "dt changed since the forward pass%s");
+    MultiStepCall scope(c, K > 1);
     int rc = begin_call(c);
     if (rc) return rc;
     {

@@ -7,8 +7,9 @@ most max(64, n / 16) pairs of the last build's neighbours tied. Runs of
 neighbours left equal over the planned bits are sorted in place by their full
 keys (runs of at most 64); a longer run makes the full sort run on the device,
 after which the plans cover the deepest split (the key bits that separate every
-pair of neighbours) for 8 calls. Whatever the plan, accepted-node counts must
-equal the oracle's and the forces must not change."""
+pair of neighbours) for 8 calls. Calls of several steps always cover the
+deepest split. Whatever the plan, accepted-node counts must equal the oracle's
+and the forces must not change."""
 import numpy as np
 import pytest
 
@@ -158,3 +159,29 @@ def test_short_plan_runs_in_the_second_word(nb, orc):
     with nb.Engine() as fresh:
         acc_full, cnt_full = fresh.barnes_hut(deeper, mt, counts=True)
     assert np.array_equal(acc, acc_full) and np.array_equal(cnt, cnt_full)
+
+
+def test_calls_of_several_steps_plan_the_deepest_split(nb, orc):
+    """A call of several steps replays one captured step while the state drifts,
+    so it sorts the passes that cover the last build's deepest split; a single
+    step or force pass sorts the fewer passes of sort_next_passes."""
+    pos, vel, mass = nb.generate(20000, gen_type=2, size=1024.0, seed=5)
+    with nb.Engine(precision=nb.PRECISION_FP64) as e:
+        e.barnes_hut(pos, mass)
+        st = e.stats()
+        split, plan = st["sort_split_bits"], st["sort_next_passes"]
+        assert plan < planned_passes(split)
+        e.set_particles(pos, vel, mass)
+        e.step(2)
+        st = e.stats()
+        assert st["sort_passes"] == planned_passes(split)
+        after_two, nxt = e.get_particles(), st["sort_next_passes"]
+        e.step(1)
+        assert e.stats()["sort_passes"] == nxt
+    with nb.Engine(precision=nb.PRECISION_FP64) as ref:  # the same steps on the full sort's trees
+        ref.set_graphs(False)
+        ref.set_particles(pos, vel, mass)
+        ref.step(1)
+        ref.step(1)
+        p2, v2 = ref.get_particles()
+    assert np.array_equal(after_two[0], p2) and np.array_equal(after_two[1], v2)
