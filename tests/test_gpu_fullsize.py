@@ -9,8 +9,8 @@ magnitude and the second key word decides most of the tree.
 - Over all N particles: the MIXED and FP64 forms accept the same nodes for every
   particle (both make the reference's decisions), the counts add up to the
   interaction statistic, and MIXED stays within p99 1e-5 of the FP64 form.
-- With damping on the sample; and the sphere of 100,000 particles, every
-  particle against the oracle."""
+- With damping on the sample; the reference's FLOAT build on the sample; and
+  the sphere of 100,000 particles, every particle against the oracle."""
 import numpy as np
 import pytest
 
@@ -86,6 +86,19 @@ def test_damped_sample_against_oracle(states, sample, eng, orc):
     acc, cnt = eng.barnes_hut(pos, mass, damping=True, theta=0.5, counts=True)
     ra, rc = orc.forces(pos, mass, 0.5, damping=True, sample=sample)
     assert np.array_equal(cnt[sample], rc)
+    assert np.percentile(rel(acc[sample], ra), 99) <= P99_MIXED
+
+
+@pytest.mark.parametrize("state", ["initial", "evolved"])
+def test_float_build_sample_against_oracle(nb, states, sample, orc, state):
+    """The reference's FLOAT build (datatype_bytes = 4) at the headline size: the
+    oracle's FLOAT path walks the seeded sample through its float tree; the
+    accepted-node counts are equal and the MIXED forces within p99 1e-5."""
+    pos, mass = states[state]
+    with nb.Engine(datatype_bytes=4) as e:
+        acc, cnt = e.barnes_hut(pos, mass, theta=0.5, counts=True)
+    ra, rc = orc.forces(pos, mass, 0.5, sample=sample, single=True)
+    assert np.array_equal(cnt[sample], rc), f"{np.count_nonzero(cnt[sample] != rc)} sampled particles differ"
     assert np.percentile(rel(acc[sample], ra), 99) <= P99_MIXED
 
 
