@@ -535,6 +535,24 @@ struct KeyView {
 
 __device__ inline int level_of(int delta) { return min(delta / 3, kMaxLevels); }
 
+// KeyView::delta(i, j) for one i, with i's first key word and system held in
+// registers (the kernel's stores could alias the keys, so the compiler would
+// load them again for every call); the deeper words only where first words agree.
+struct DeltaFrom {
+    const KeyView &kv;
+    int i;
+    uint64_t a1;
+    uint32_t si;
+    __device__ DeltaFrom(const KeyView &v, int at) : kv(v), i(at), a1(v.k1[at]), si(v.sys ? v.sys[at] : 0u) {}
+    __device__ int operator()(int j) const {
+        if (j < 0 || j >= kv.n) return -1;
+        if (kv.sys && kv.sys[j] != si) return -1;
+        const uint64_t b1 = kv.k1[j];
+        if (a1 != b1) return __clzll(a1 ^ b1) - 1;
+        return kv.delta(i, j);
+    }
+};
+
 __global__ void k_radix_tree(KeyView kv, int32_t *__restrict__ bleft, int32_t *__restrict__ bright,
                              int32_t *__restrict__ bparent, int32_t *__restrict__ leaf_bparent,
                              int32_t *__restrict__ bdelta, uint32_t *max_prefix_bits, uint32_t *pair_passes) {
@@ -543,7 +561,7 @@ __global__ void k_radix_tree(KeyView kv, int32_t *__restrict__ bleft, int32_t *_
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = kv.n;
     // the deepest split: key bits that separate every pair of neighbours
-    const int dn = i < n - 1 ? kv.delta(i, i + 1) : -1;
+    const int dn = i < n - 1 ? DeltaFrom(kv, i)(i + 1) : -1;
     const int wmax = __reduce_max_sync(0xffffffffu, dn);
     if ((threadIdx.x & 31) == 0 && wmax >= 0) atomicMax(max_prefix_bits, (uint32_t)wmax + 1u);
     // the pairs by the sort passes that separate them (the next build's plan):
@@ -566,19 +584,21 @@ __global__ void k_radix_tree(KeyView kv, int32_t *__restrict__ bleft, int32_t *_
         return;
     }
     const bool seg_root = i == 0 || (kv.sys && kv.sys[i - 1] != kv.sys[i]);
-    int d = (kv.delta(i, i + 1) - kv.delta(i, i - 1)) >= 0 ? 1 : -1;
-    int dmin = kv.delta(i, i - d);
+    const DeltaFrom di(kv, i);
+    const int dprev = di(i - 1);
+    int d = (dn - dprev) >= 0 ? 1 : -1;
+    int dmin = d > 0 ? dprev : dn;  // delta(i, i - d)
     int lmax = 2;
-    while (kv.delta(i, i + lmax * d) > dmin) lmax <<= 1;
+    while (di(i + lmax * d) > dmin) lmax <<= 1;
     int l = 0;
     for (int t = lmax >> 1; t >= 1; t >>= 1)
-        if (kv.delta(i, i + (l + t) * d) > dmin) l += t;
+        if (di(i + (l + t) * d) > dmin) l += t;
     int j = i + l * d;
-    int dnode = kv.delta(i, j);
+    int dnode = di(j);
     int s = 0, t = l;
     do {
         t = (t + 1) >> 1;
-        if (kv.delta(i, i + (s + t) * d) > dnode) s += t;
+        if (di(i + (s + t) * d) > dnode) s += t;
     } while (t > 1);
     int gamma = i + s * d + min(d, 0);
     int lo = min(i, j), hi = max(i, j);
