@@ -663,32 +663,73 @@ __global__ void k_collapse(const int32_t *__restrict__ bleft, const int32_t *__r
     if (i >= m || !flag[i]) return;
     const int id = (int)head_id[i];
     const int L = level_of(bdelta[i]);
-    // In-order walk over the same-level binary nodes (at most 7 of them):
-    // a frame visits its left child, then its right child.
-    int fnode[8], fstate[8];
-    int fs = 0, nch = 0, nint = 0;
-    fnode[0] = (int)i; fstate[0] = 0; fs = 1;
-    while (fs > 0) {
-        const int x = fnode[fs - 1];
-        if (fstate[fs - 1] == 2) { fs--; continue; }
-        const int ch = fstate[fs - 1] == 0 ? bleft[x] : bright[x];
-        fstate[fs - 1]++;
-        if (ch >= 0 && level_of(bdelta[ch]) == L) {
-            if (fs < 8) { fnode[fs] = ch; fstate[fs] = 0; fs++; }
-            else atomicOr(&sc->status, kStatusCapacity);
-        } else if (nch < 8) {
-            if (ch < 0) {
-                ochild[8 * id + nch] = ch;
-                leaf_oparent[~ch] = id;
-            } else {
-                const int cid = (int)head_id[ch];
-                ochild[8 * id + nch] = cid;
-                oparent[cid] = id;
-                nint++;
-            }
-            nch++;
-        } else {
+    int nch = 0, nint = 0;
+    // A child that is no binary node of this octree level becomes a child of
+    // the octree node, in order.
+    auto emit = [&](int ch) {
+        if (nch >= 8) {
             atomicOr(&sc->status, kStatusCapacity);
+            return;
+        }
+        if (ch < 0) {
+            ochild[8 * id + nch] = ch;
+            leaf_oparent[~ch] = id;
+        } else {
+            const int cid = (int)head_id[ch];
+            ochild[8 * id + nch] = cid;
+            oparent[cid] = id;
+            nint++;
+        }
+        nch++;
+    };
+    auto same_level = [&](int ch) { return ch >= 0 && level_of(bdelta[ch]) == L; };
+    if (L >= kMaxLevels) {
+        // The capped level (keys equal over every word: coincident particles,
+        // reported as such) can nest deeper: an in-order walk with a stack, a
+        // frame visiting its left child, then its right child.
+        int fnode[8], fstate[8];
+        int fs = 1;
+        fnode[0] = (int)i;
+        fstate[0] = 0;
+        while (fs > 0) {
+            const int x = fnode[fs - 1];
+            if (fstate[fs - 1] == 2) { fs--; continue; }
+            const int ch = fstate[fs - 1] == 0 ? bleft[x] : bright[x];
+            fstate[fs - 1]++;
+            if (same_level(ch)) {
+                if (fs < 8) { fnode[fs] = ch; fstate[fs] = 0; fs++; }
+                else atomicOr(&sc->status, kStatusCapacity);
+            } else {
+                emit(ch);
+            }
+        }
+    } else {
+        // In-order walk over the same-level binary nodes. Their prefix lengths grow
+        // strictly downwards and stay within the level's 3 key bits, so the walk is
+        // at most 3 binary nodes deep: unrolled, with nothing in local memory.
+        const int c1[2] = {bleft[i], bright[i]};
+    #pragma unroll
+        for (int a = 0; a < 2; a++) {
+            const int x = c1[a];
+            if (!same_level(x)) {
+                emit(x);
+                continue;
+            }
+            const int c2[2] = {bleft[x], bright[x]};
+    #pragma unroll
+            for (int b = 0; b < 2; b++) {
+                const int y = c2[b];
+                if (!same_level(y)) {
+                    emit(y);
+                    continue;
+                }
+                const int c3[2] = {bleft[y], bright[y]};
+    #pragma unroll
+                for (int c = 0; c < 2; c++) {
+                    if (same_level(c3[c])) atomicOr(&sc->status, kStatusCapacity);  // deeper than 3: malformed
+                    else emit(c3[c]);
+                }
+            }
         }
     }
     ometa[id] = L | (min(nch, 8) << 8) | (min(nint, 8) << 12);
