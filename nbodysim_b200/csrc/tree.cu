@@ -87,14 +87,27 @@ __global__ void k_bbox(const double *__restrict__ pos, const double *__restrict_
         }
     }
     __syncthreads();
-    if (!s_last || wid != 0) return;
+    if (!s_last) return;
+    // The last block reduces every block's partials: each thread takes whole
+    // rows (seven independent loads), then a block reduction.
     __threadfence();
-    double r[7];
-    for (int k = 0; k < 7; k++) {
-        double acc = INFINITY;
-        for (uint32_t b = lane; b < gridDim.x; b += 32) acc = fmin(acc, __ldcg(&partial[7 * b + k]));
-        r[k] = warp_min(acc);
+    double acc[7];
+#pragma unroll
+    for (int k = 0; k < 7; k++) acc[k] = INFINITY;
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 7; k++) acc[k] = fmin(acc[k], __ldcg(&partial[7 * b + k]));
     }
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+        const double m = warp_min(acc[k]);
+        if (lane == 0) s_red[k][wid] = m;
+    }
+    __syncthreads();
+    if (wid != 0) return;
+    double r[7];
+#pragma unroll
+    for (int k = 0; k < 7; k++) r[k] = warp_min(lane < nw ? s_red[k][lane] : INFINITY);
     if (lane == 0 && keep_root) {
         sc->max_vel_bits = (unsigned long long)__double_as_longlong(sqrt(-r[6]));
         sc->ticket = 0;
